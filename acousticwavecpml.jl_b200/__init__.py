@@ -1,0 +1,20 @@
+"""B200-native CPML acoustic time stepping behind AcousticWaveCPML.jl's API.
+
+Python mirror of the reference's public surface for the GPU solvers:
+``Acoustic2D_CUDA.solve2D``, ``Acoustic3D_CUDA.solve3D``, ``Sources``,
+``Receivers``, ``rickersource1D`` and ``calc_Kab_CPML``. The compute runs in
+libawcpml.so (hand-written sm_100a kernels behind the C ABI of
+include/awcpml.h); ``julia/AcousticWaveCPML_B200.jl`` is the equivalent Julia
+shim that `ccall`s the same library.
+
+The directory name is not a Python identifier; load it with
+``__graft_entry__.load_package()`` (registers it as ``acousticwavecpml_b200``).
+"""
+from . import Acoustic2D_CUDA, Acoustic3D_CUDA  # noqa: F401
+from ._lib import AWC_F32, AWC_F64, AwcError, AwcInvalidArgument, Problem  # noqa: F401
+from .core import Context, Plan, default_context, prepare  # noqa: F401
+from .utils import Receivers, Sources, calc_Kab_CPML, rickersource1D  # noqa: F401
+
+__all__ = ["Acoustic2D_CUDA", "Acoustic3D_CUDA", "Sources", "Receivers", "rickersource1D",
+           "calc_Kab_CPML", "Context", "Plan", "prepare", "default_context", "Problem",
+           "AwcError", "AwcInvalidArgument", "AWC_F32", "AWC_F64"]

@@ -1,0 +1,772 @@
+// awc_api.cu — host side of the C ABI declared in include/awcpml.h.
+//
+// Responsibilities: argument validation with the reference's error cases
+// (positions inside the model, src/shared/acoustic_3D_xPU.jl:281,289; halo
+// small enough for the band index arithmetic of :12,:68), the FP64 CPML
+// coefficient setup (src/utils.jl:19-57), device buffers, the per-step launch
+// sequence of forward! (:124-167) and its capture into CUDA graphs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <unordered_map>
+#include <utility>
+#include <vector>
+
+#include "../../include/awcpml.h"
+#include "awc_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_thread_err;
+
+int set_err(std::string* dst, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_thread_err = buf;
+  if (dst) *dst = buf;
+  return code;
+}
+
+#define CUDA_TRY(dst, call)                                                              \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      return set_err(dst, e_ == cudaErrorMemoryAllocation ? AWC_ERR_OOM : AWC_ERR_CUDA,  \
+                     "%s failed: %s", #call, cudaGetErrorString(e_));                    \
+    }                                                                                    \
+  } while (0)
+
+// CPML profile restated from calc_Kab_CPML (src/utils.jl:19-57), FP64.
+void kab(int32_t halo, double dt, double npower, double d0, double alpha_max, double K_max,
+         bool halfgrid, double* a_l, double* a_r, double* bK_l, double* bK_r) {
+  const int64_t n = halo + (halfgrid ? 1 : 0);
+  if (n == 0) return;
+  const double shift = halfgrid ? 0.5 : 0.0;
+  std::vector<double> dist(n);
+  // LinRange(0-shift, n-shift-1, n): element j = (1-t)*start + t*stop, t = j/(n-1)
+  const double lo = 0.0 - shift, hi = (double)n - shift - 1.0;
+  for (int64_t j = 0; j < n; ++j) {
+    if (n == 1) {
+      dist[j] = lo;
+    } else {
+      const double t = (double)j / (double)(n - 1);
+      dist[j] = (1.0 - t) * lo + t * hi;
+    }
+  }
+  if (halfgrid) dist[0] = 0.0;  // the staggered profile starts on the edge node
+  auto powN = [npower](double x) { return npower == 2.0 ? x * x : std::pow(x, npower); };
+  for (int64_t m = 0; m < n; ++m) {
+    for (int side = 0; side < 2; ++side) {
+      // left side reads the distance profile reversed
+      const double r = (side == 0 ? dist[n - 1 - m] : dist[m]) / (double)halo;
+      const double rN = powN(r);
+      const double d = d0 * rN;
+      const double alpha = alpha_max * (1.0 - r);
+      const double K = 1.0 + (K_max - 1.0) * rN;
+      const double b = std::exp(-(d / K + alpha) * dt);
+      const double a = d * (b - 1.0) / (K * (d + K * alpha));
+      (side == 0 ? a_l : a_r)[m] = a;
+      (side == 0 ? bK_l : bK_r)[m] = b / K;
+    }
+  }
+}
+
+int validate(const awc_problem* p, std::string* err) {
+  if (!p) return set_err(err, AWC_ERR_INVALID, "problem is NULL");
+  if (p->ndim != 2 && p->ndim != 3)
+    return set_err(err, AWC_ERR_INVALID, "ndim must be 2 or 3 (got %d)", p->ndim);
+  if (p->precision != AWC_F32 && p->precision != AWC_F64)
+    return set_err(err, AWC_ERR_INVALID, "precision must be AWC_F32 or AWC_F64");
+  const int64_t n[3] = {p->nx, p->ny, p->ndim == 3 ? p->nz : 3};
+  for (int a = 0; a < p->ndim; ++a) {
+    if (n[a] < 3 || n[a] > (int64_t)1 << 30)
+      return set_err(err, AWC_ERR_INVALID, "grid size along axis %d must be in [3, 2^30]", a);
+  }
+  if (p->ndim == 2 && p->nz != 1) return set_err(err, AWC_ERR_INVALID, "2D problems need nz = 1");
+  if (p->halo < 0) return set_err(err, AWC_ERR_INVALID, "halo must be >= 0");
+  for (int a = 0; a < p->ndim; ++a) {
+    // right-band ψ reads pcur[i + n - halo - 2] for i = 1 (acoustic_3D_xPU.jl:12)
+    if (p->halo > n[a] - 2)
+      return set_err(err, AWC_ERR_INVALID, "halo %d too large for %lld nodes on axis %d",
+                     p->halo, (long long)n[a], a);
+  }
+  const double d[3] = {p->dx, p->dy, p->ndim == 3 ? p->dz : 1.0};
+  for (int a = 0; a < p->ndim; ++a)
+    if (!(d[a] > 0.0) || !std::isfinite(d[a]))
+      return set_err(err, AWC_ERR_INVALID, "grid spacing must be positive and finite");
+  if (!(p->dt > 0.0) || !std::isfinite(p->dt))
+    return set_err(err, AWC_ERR_INVALID, "dt must be positive and finite");
+  if (p->nt < 0 || p->nt > ((int64_t)1 << 31))
+    return set_err(err, AWC_ERR_INVALID, "nt out of range");
+  if (p->nsrc < 0 || p->nrec < 0 || p->nsrc > (1 << 30) || p->nrec > (1 << 30))
+    return set_err(err, AWC_ERR_INVALID, "nsrc/nrec out of range");
+  return AWC_OK;
+}
+
+int check_positions(const awc_problem* p, const int64_t* pos, int64_t cnt, const char* what,
+                    std::string* err) {
+  if (cnt > 0 && !pos) return set_err(err, AWC_ERR_INVALID, "%s positions are NULL", what);
+  const int64_t n[3] = {p->nx, p->ny, p->nz};
+  for (int64_t s = 0; s < cnt; ++s)
+    for (int a = 0; a < p->ndim; ++a) {
+      const int64_t v = pos[s + cnt * a];
+      if (v < 1 || v > n[a])
+        return set_err(err, AWC_ERR_INVALID, "At least one %s is not inside the model!", what);
+    }
+  return AWC_OK;
+}
+
+int64_t node_of(const awc_problem* p, const int64_t* pos, int64_t cnt, int64_t s) {
+  const int64_t i = pos[s] - 1, j = pos[s + cnt] - 1, k = p->ndim == 3 ? pos[s + 2 * cnt] - 1 : 0;
+  return i + p->nx * (j + p->ny * k);
+}
+
+}  // namespace
+
+struct awc_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  float last_run_ms = 0.f;
+  std::vector<awc_plan*> cache;  // plans reused by awc_forward, most recent last
+};
+
+struct awc_plan {
+  awc_ctx* ctx = nullptr;
+  awc_problem p{};
+  size_t esz = 0;  // bytes per element of T
+  int64_t N = 0;   // nodes
+  // device buffers
+  void* buf[3] = {nullptr, nullptr, nullptr};
+  void* fact = nullptr;
+  void* psi[3][2][2] = {};  // [axis][side][old/new parity]
+  void* xi[3][2] = {};
+  void* coef = nullptr;  // packed coefficients in T
+  int64_t* src_node = nullptr;
+  int32_t* src_off = nullptr;
+  int32_t* src_ids = nullptr;
+  int32_t nsrc_nodes = 0;
+  void* stf = nullptr;  // [nt][nsrc]
+  int64_t* rec_node = nullptr;
+  void* traces = nullptr;  // [nt][nrec]
+  double* staging = nullptr;
+  int64_t staging_len = 0;
+  std::vector<void*> allocs;
+  // run state
+  int64_t step = 0;
+  int32_t active[3][2] = {};
+  int32_t by = 8, zchunk = 0;
+  std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
+  uint64_t graph_key = 0;  // launch configuration the graphs were captured with
+
+  int alloc(void** out, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(out, bytes);
+    if (e != cudaSuccess) {
+      *out = nullptr;
+      cudaGetLastError();
+      return set_err(&ctx->err, e == cudaErrorMemoryAllocation ? AWC_ERR_OOM : AWC_ERR_CUDA,
+                     "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    allocs.push_back(*out);
+    return AWC_OK;
+  }
+  void drop_graphs() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+    graphs.clear();
+  }
+  ~awc_plan() {
+    drop_graphs();
+    for (void* a : allocs) cudaFree(a);
+  }
+};
+
+namespace {
+
+int64_t cross_section(const awc_problem* p, int axis) {
+  const int64_t nz = p->ndim == 3 ? p->nz : 1;
+  return axis == 0 ? p->ny * nz : axis == 1 ? p->nx * nz : p->nx * p->ny;
+}
+
+// Allocates every device buffer of a plan (shape only, contents undefined).
+int plan_alloc(awc_plan* P) {
+  const awc_problem* p = &P->p;
+  const int64_t h = p->halo;
+  P->esz = p->precision == AWC_F64 ? 8 : 4;
+  P->N = p->nx * p->ny * (p->ndim == 3 ? p->nz : 1);
+  int rc;
+  for (int b = 0; b < 3; ++b)
+    if ((rc = P->alloc(&P->buf[b], P->N * P->esz))) return rc;
+  if ((rc = P->alloc(&P->fact, P->N * P->esz))) return rc;
+  for (int a = 0; a < p->ndim; ++a)
+    for (int s = 0; s < 2; ++s) {
+      const int64_t cs = cross_section(p, a);
+      for (int par = 0; par < 2; ++par)
+        if ((rc = P->alloc(&P->psi[a][s][par], (h + 1) * cs * P->esz))) return rc;
+      if ((rc = P->alloc(&P->xi[a][s], h * cs * P->esz))) return rc;
+    }
+  if ((rc = P->alloc(&P->coef, awc_coeffs_len(p) * P->esz))) return rc;
+  if ((rc = P->alloc((void**)&P->src_node, std::max<int64_t>(p->nsrc, 1) * 8))) return rc;
+  if ((rc = P->alloc((void**)&P->src_off, (std::max<int64_t>(p->nsrc, 1) + 1) * 4))) return rc;
+  if ((rc = P->alloc((void**)&P->src_ids, std::max<int64_t>(p->nsrc, 1) * 4))) return rc;
+  if ((rc = P->alloc(&P->stf, std::max<int64_t>(p->nt * p->nsrc, 1) * P->esz))) return rc;
+  if ((rc = P->alloc((void**)&P->rec_node, std::max<int64_t>(p->nrec, 1) * 8))) return rc;
+  if ((rc = P->alloc(&P->traces, std::max<int64_t>(p->nt * p->nrec, 1) * P->esz))) return rc;
+  P->staging_len = std::max<int64_t>(P->N, p->nt * p->nrec);
+  if ((rc = P->alloc((void**)&P->staging, P->staging_len * 8))) return rc;
+  return AWC_OK;
+}
+
+template <typename T>
+void to_T(const double* src, std::vector<unsigned char>& out, int64_t n) {
+  out.resize(n * sizeof(T));
+  T* d = reinterpret_cast<T*>(out.data());
+  for (int64_t c = 0; c < n; ++c) d[c] = (T)src[c];
+}
+
+// Uploads the inputs of one shot into an allocated plan. The copies are
+// stream-ordered on the context stream.
+int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int64_t* possrcs,
+                const double* dt2srctf, const int64_t* posrecs) {
+  awc_ctx* C = P->ctx;
+  const awc_problem* p = &P->p;
+  std::string* err = &C->err;
+  cudaStream_t st = C->stream;
+  const int64_t h = p->halo, nt = p->nt, nsrc = p->nsrc, nrec = p->nrec;
+  const bool f64 = p->precision == AWC_F64;
+  // fact = dt^2 vel^2 on the device in FP64
+  CUDA_TRY(err, cudaMemcpyAsync(P->staging, vel, P->N * 8, cudaMemcpyHostToDevice, st));
+  {
+    const int threads = 256;
+    const int64_t want = (P->N + threads - 1) / threads;
+    const int blocks = (int)std::min<int64_t>(want, (int64_t)C->num_sms * 16);
+    const double dt2 = p->dt * p->dt;
+    if (f64)
+      awc::make_fact<double><<<blocks, threads, 0, st>>>(P->staging, (double*)P->fact, dt2, P->N);
+    else
+      awc::make_fact<float><<<blocks, threads, 0, st>>>(P->staging, (float*)P->fact, dt2, P->N);
+    CUDA_TRY(err, cudaGetLastError());
+  }
+  // coefficients (and which band sides are live)
+  const int64_t clen = awc_coeffs_len(p);
+  std::vector<unsigned char> tmp;
+  if (f64) to_T<double>(coeffs, tmp, clen); else to_T<float>(coeffs, tmp, clen);
+  CUDA_TRY(err, cudaMemcpyAsync(P->coef, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(err, cudaStreamSynchronize(st));  // tmp is reused below
+  for (int a = 0; a < p->ndim; ++a) {
+    const double* blk = coeffs + a * (8 * h + 4);
+    for (int s = 0; s < 2; ++s) {
+      // a side whose every a is 0 and every b/K is 1 keeps ψ = ξ = 0 for ever
+      // (the free top, acoustic_3D_xPU.jl:225-230); its updates are skipped.
+      bool trivial = true;
+      for (int64_t m = 0; m < h; ++m)
+        trivial = trivial && blk[s * h + m] == 0.0 && blk[2 * h + s * h + m] == 1.0;
+      const double* hb = blk + 4 * h;
+      for (int64_t m = 0; m < h + 1; ++m)
+        trivial = trivial && hb[s * (h + 1) + m] == 0.0 && hb[2 * (h + 1) + s * (h + 1) + m] == 1.0;
+      P->active[a][s] = (h > 0 && !trivial) ? 1 : 0;
+    }
+  }
+  // sources grouped by node in first-appearance order, summed in source order
+  {
+    std::vector<int64_t> nodes;
+    std::vector<std::vector<int32_t>> groups;
+    std::unordered_map<int64_t, int32_t> where;
+    for (int64_t s = 0; s < nsrc; ++s) {
+      const int64_t nd = node_of(p, possrcs, nsrc, s);
+      auto it = where.find(nd);
+      if (it == where.end()) {
+        where.emplace(nd, (int32_t)nodes.size());
+        nodes.push_back(nd);
+        groups.push_back({(int32_t)s});
+      } else {
+        groups[it->second].push_back((int32_t)s);
+      }
+    }
+    std::vector<int32_t> off(1, 0), ids;
+    for (auto& g : groups) {
+      ids.insert(ids.end(), g.begin(), g.end());
+      off.push_back((int32_t)ids.size());
+    }
+    P->nsrc_nodes = (int32_t)nodes.size();
+    if (!nodes.empty()) {
+      CUDA_TRY(err, cudaMemcpyAsync(P->src_node, nodes.data(), nodes.size() * 8,
+                                    cudaMemcpyHostToDevice, st));
+      CUDA_TRY(err, cudaMemcpyAsync(P->src_ids, ids.data(), ids.size() * 4,
+                                    cudaMemcpyHostToDevice, st));
+    }
+    CUDA_TRY(err, cudaMemcpyAsync(P->src_off, off.data(), off.size() * 4,
+                                  cudaMemcpyHostToDevice, st));
+    // stf rows: [it][s] from the column-major (nt x nsrc) input
+    std::vector<double> rows((size_t)std::max<int64_t>(nt * nsrc, 1), 0.0);
+    for (int64_t s = 0; s < nsrc; ++s)
+      for (int64_t t = 0; t < nt; ++t) rows[t * nsrc + s] = dt2srctf[t + nt * s];
+    if (f64) to_T<double>(rows.data(), tmp, nt * nsrc); else to_T<float>(rows.data(), tmp, nt * nsrc);
+    if (nt * nsrc > 0)
+      CUDA_TRY(err, cudaMemcpyAsync(P->stf, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, st));
+    std::vector<int64_t> rn(std::max<int64_t>(nrec, 1));
+    for (int64_t r = 0; r < nrec; ++r) rn[r] = node_of(p, posrecs, nrec, r);
+    if (nrec > 0)
+      CUDA_TRY(err, cudaMemcpyAsync(P->rec_node, rn.data(), nrec * 8, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(err, cudaStreamSynchronize(st));  // host vectors go out of scope
+  }
+  return AWC_OK;
+}
+
+template <typename T>
+awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
+  const awc_problem* p = &P->p;
+  awc::StepParams<T> S{};
+  T* b[3] = {(T*)P->buf[0], (T*)P->buf[1], (T*)P->buf[2]};
+  // step it (0-based) reads pold = buf[it%3], pcur = buf[(it+1)%3] and writes
+  // pnew = buf[(it+2)%3]: the (pold, pcur, pnew) <- (pcur, pnew, pold)
+  // rotation of forward! (acoustic_3D_xPU.jl:166)
+  S.pold = b[it % 3];
+  S.pcur = b[(it + 1) % 3];
+  S.pnew = b[(it + 2) % 3];
+  S.fact = (const T*)P->fact;
+  S.nx = (int32_t)p->nx;
+  S.ny = (int32_t)p->ny;
+  S.nz = (int32_t)(p->ndim == 3 ? p->nz : 1);
+  S.halo = p->halo;
+  const double d[3] = {p->dx, p->dy, p->ndim == 3 ? p->dz : 1.0};
+  for (int a = 0; a < 3; ++a) {
+    S.inv_d[a] = (T)(1.0 / d[a]);
+    S.inv_d2[a] = (T)(1.0 / (d[a] * d[a]));
+  }
+  const int64_t h = p->halo;
+  const T* cf = (const T*)P->coef;
+  for (int a = 0; a < p->ndim; ++a) {
+    const T* blk = cf + a * (8 * h + 4);
+    for (int s = 0; s < 2; ++s) {
+      awc::BandSide<T>& B = S.band[a][s];
+      B.psi_old = (const T*)P->psi[a][s][it & 1];
+      B.psi_new = (T*)P->psi[a][s][(it + 1) & 1];
+      B.xi = (T*)P->xi[a][s];
+      B.a = blk + s * h;
+      B.bK = blk + 2 * h + s * h;
+      B.ah = blk + 4 * h + s * (h + 1);
+      B.bKh = blk + 4 * h + 2 * (h + 1) + s * (h + 1);
+      S.active[a][s] = P->active[a][s];
+    }
+    const int64_t n = a == 0 ? p->nx : a == 1 ? p->ny : p->nz;
+    S.first_r[a] = (int32_t)std::max<int64_t>(n - h - 1, h + 1);
+  }
+  S.zchunk = P->zchunk;
+  S.it = (int32_t)it;
+  return S;
+}
+
+template <typename T>
+awc::Io<T> io_params(const awc_plan* P) {
+  awc::Io<T> io{};
+  io.src_node = P->src_node;
+  io.src_off = P->src_off;
+  io.src_ids = P->src_ids;
+  io.nsrc_nodes = P->nsrc_nodes;
+  io.stf = (const T*)P->stf;
+  io.nsrc = (int32_t)P->p.nsrc;
+  io.rec_node = P->rec_node;
+  io.nrec = (int32_t)P->p.nrec;
+  io.traces = (T*)P->traces;
+  return io;
+}
+
+template <typename T>
+int launch_step(awc_plan* P, int64_t it, cudaStream_t st) {
+  const awc_problem* p = &P->p;
+  awc::StepParams<T> S = step_params<T>(P, it);
+  const int ix = (int)(p->nx - 2), iy = (int)(p->ny - 2);
+  if (p->ndim == 3) {
+    const int iz = (int)(p->nz - 2);
+    dim3 grid((ix + 31) / 32, (iy + P->by - 1) / P->by, (iz + P->zchunk - 1) / P->zchunk);
+    switch (P->by) {
+      case 4: awc::step3d<T, 4><<<grid, dim3(32, 4), 0, st>>>(S); break;
+      case 8: awc::step3d<T, 8><<<grid, dim3(32, 8), 0, st>>>(S); break;
+      case 16: awc::step3d<T, 16><<<grid, dim3(32, 16), 0, st>>>(S); break;
+      default: return set_err(&P->ctx->err, AWC_ERR_INVALID, "unsupported tile height %d", P->by);
+    }
+  } else {
+    dim3 block(32, 8);
+    dim3 grid((ix + 31) / 32, (iy + 7) / 8);
+    awc::step2d<T><<<grid, block, 0, st>>>(S);
+  }
+  if (p->nsrc > 0 || p->nrec > 0) {
+    const int threads = (int)std::min<int64_t>(1024, ((std::max(p->nsrc, p->nrec) + 31) / 32) * 32);
+    awc::inject_record<T><<<1, threads, 0, st>>>(S.pnew, io_params<T>(P), (int)it);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return set_err(&P->ctx->err, AWC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  return AWC_OK;
+}
+
+int launch_range(awc_plan* P, int64_t start, int64_t n, cudaStream_t st) {
+  for (int64_t it = start; it < start + n; ++it) {
+    int rc = P->p.precision == AWC_F64 ? launch_step<double>(P, it, st) : launch_step<float>(P, it, st);
+    if (rc) return rc;
+  }
+  return AWC_OK;
+}
+
+uint64_t config_key(const awc_plan* P) {
+  uint64_t k = (uint64_t)P->by | ((uint64_t)P->zchunk << 8);
+  for (int a = 0; a < 3; ++a)
+    for (int s = 0; s < 2; ++s) k |= (uint64_t)P->active[a][s] << (40 + 2 * a + s);
+  return k;
+}
+
+int get_graph(awc_plan* P, int64_t start, int64_t n, cudaGraphExec_t* out) {
+  awc_ctx* C = P->ctx;
+  const uint64_t key = config_key(P);
+  if (key != P->graph_key) {
+    P->drop_graphs();
+    P->graph_key = key;
+  }
+  auto f = P->graphs.find({start, n});
+  if (f != P->graphs.end()) {
+    *out = f->second;
+    return AWC_OK;
+  }
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(&C->err, cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = launch_range(P, start, n, C->stream);
+  cudaError_t e = cudaStreamEndCapture(C->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess)
+    return set_err(&C->err, AWC_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+  cudaGraphExec_t ex = nullptr;
+  e = cudaGraphInstantiate(&ex, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess)
+    return set_err(&C->err, AWC_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+  P->graphs[{start, n}] = ex;
+  *out = ex;
+  return AWC_OK;
+}
+
+// Default launch shape: tile 32 x 8 columns; z chunks so that one wave of
+// resident blocks covers the grid (148 SMs on B200).
+void default_tuning(awc_plan* P) {
+  const awc_problem* p = &P->p;
+  P->by = 8;
+  if (p->ndim != 3) {
+    P->zchunk = 1;
+    return;
+  }
+  const int64_t ix = p->nx - 2, iy = p->ny - 2, iz = p->nz - 2;
+  const int64_t tiles = ((ix + 31) / 32) * ((iy + P->by - 1) / P->by);
+  int occ = 0;
+  if (p->precision == AWC_F64)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, awc::step3d<double, 8>, 256, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, awc::step3d<float, 8>, 256, 0);
+  if (occ <= 0) occ = 4;
+  const int64_t resident = (int64_t)P->ctx->num_sms * occ;
+  int64_t nch = std::max<int64_t>(1, resident / std::max<int64_t>(tiles, 1));
+  nch = std::min<int64_t>(nch, iz);
+  P->zchunk = (int32_t)((iz + nch - 1) / nch);
+}
+
+int forward_impl(awc_ctx* C, const awc_problem* p, const double* vel, const double* coeffs,
+                 const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
+                 awc_plan** out) {
+  std::string* err = &C->err;
+  int rc;
+  if ((rc = validate(p, err))) return rc;
+  if (!vel || !coeffs) return set_err(err, AWC_ERR_INVALID, "vel/coeffs are NULL");
+  if (p->nsrc > 0 && p->nt > 0 && !dt2srctf)
+    return set_err(err, AWC_ERR_INVALID, "dt2srctf is NULL");
+  if ((rc = check_positions(p, possrcs, p->nsrc, "source", err))) return rc;
+  if ((rc = check_positions(p, posrecs, p->nrec, "receiver", err))) return rc;
+  awc_plan* P = new awc_plan();
+  P->ctx = C;
+  P->p = *p;
+  if (p->ndim == 2) P->p.nz = 1;
+  CUDA_TRY(err, cudaSetDevice(C->device));
+  if ((rc = plan_alloc(P)) || (rc = plan_upload(P, vel, coeffs, possrcs, dt2srctf, posrecs))) {
+    delete P;
+    return rc;
+  }
+  default_tuning(P);
+  *out = P;
+  return awc_plan_reset(P);
+}
+
+bool same_shape(const awc_problem& a, const awc_problem& b) {
+  return a.ndim == b.ndim && a.precision == b.precision && a.nx == b.nx && a.ny == b.ny &&
+         (a.ndim == 2 || a.nz == b.nz) && a.halo == b.halo && a.nt == b.nt && a.nsrc == b.nsrc &&
+         a.nrec == b.nrec;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int64_t awc_coeffs_len(const awc_problem* p) {
+  if (!p || (p->ndim != 2 && p->ndim != 3) || p->halo < 0) return 0;
+  return (int64_t)p->ndim * (8 * (int64_t)p->halo + 4);
+}
+
+int awc_cpml_coeffs(int32_t halo, double dt, double npower, double d0, double alpha_max,
+                    double K_max, int32_t halfgrid, double* a_l, double* a_r, double* bK_l,
+                    double* bK_r) {
+  if (halo < 0) return set_err(nullptr, AWC_ERR_INVALID, "halo must be >= 0");
+  if ((halo > 0 || halfgrid) && (!a_l || !a_r || !bK_l || !bK_r))
+    return set_err(nullptr, AWC_ERR_INVALID, "output vectors are NULL");
+  kab(halo, dt, npower, d0, alpha_max, K_max, halfgrid != 0, a_l, a_r, bK_l, bK_r);
+  return AWC_OK;
+}
+
+int awc_problem_coeffs(const awc_problem* p, double rcoef, double f0, double vel_max,
+                       double* coeffs) {
+  int rc = validate(p, nullptr);
+  if (rc) return rc;
+  if (!coeffs) return set_err(nullptr, AWC_ERR_INVALID, "coeffs is NULL");
+  const int64_t h = p->halo;
+  const double alpha_max = M_PI * f0, npower = 2.0, K_max = 1.0;
+  const double d[3] = {p->dx, p->dy, p->dz};
+  for (int a = 0; a < p->ndim; ++a) {
+    double* blk = coeffs + a * (8 * h + 4);
+    const double thickness = (double)h * d[a];
+    const double d0 = -(npower + 1.0) * vel_max * std::log(rcoef) / (2.0 * thickness);
+    kab(p->halo, p->dt, npower, d0, alpha_max, K_max, false, blk, blk + h, blk + 2 * h, blk + 3 * h);
+    double* hb = blk + 4 * h;
+    kab(p->halo, p->dt, npower, d0, alpha_max, K_max, true, hb, hb + (h + 1), hb + 2 * (h + 1),
+        hb + 3 * (h + 1));
+    if (a == 1 && p->freetop) {
+      for (int64_t m = 0; m < h; ++m) {
+        blk[m] = 0.0;
+        blk[2 * h + m] = 1.0;
+      }
+      for (int64_t m = 0; m < h + 1; ++m) {
+        hb[m] = 0.0;
+        hb[2 * (h + 1) + m] = 1.0;
+      }
+    }
+  }
+  return AWC_OK;
+}
+
+int awc_ricker(int64_t n, const double* t, double t0, double f0, double* out) {
+  if (n < 0 || (n > 0 && (!t || !out))) return set_err(nullptr, AWC_ERR_INVALID, "bad arguments");
+  for (int64_t m = 0; m < n; ++m) {
+    const double x = M_PI * f0 * (t[m] - t0);
+    out[m] = (1.0 - 2.0 * (x * x)) * std::exp(-(x * x));
+  }
+  return AWC_OK;
+}
+
+int awc_create(awc_ctx** out, int32_t device) {
+  if (!out) return set_err(nullptr, AWC_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return set_err(nullptr, AWC_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  }
+  if (device < 0 || device >= count)
+    return set_err(nullptr, AWC_ERR_INVALID, "device %d out of range (%d devices)", device, count);
+  cudaDeviceProp prop;
+  CUDA_TRY(nullptr, cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return set_err(nullptr, AWC_ERR_NODEVICE, "device %d is sm_%d%d; this build targets sm_100a",
+                   device, prop.major, prop.minor);
+  CUDA_TRY(nullptr, cudaSetDevice(device));
+  awc_ctx* C = new awc_ctx();
+  C->device = device;
+  C->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&C->ev0) != cudaSuccess || cudaEventCreate(&C->ev1) != cudaSuccess) {
+    awc_destroy(C);
+    return set_err(nullptr, AWC_ERR_CUDA, "stream/event creation failed");
+  }
+  *out = C;
+  return AWC_OK;
+}
+
+void awc_destroy(awc_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  for (awc_plan* P : ctx->cache) delete P;
+  ctx->cache.clear();
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* awc_last_error(const awc_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_thread_err.c_str();
+}
+
+float awc_last_run_ms(const awc_ctx* ctx) { return ctx ? ctx->last_run_ms : 0.f; }
+
+void* awc_ctx_stream(const awc_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int awc_plan_create(awc_ctx* ctx, const awc_problem* p, const double* vel, const double* coeffs,
+                    const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
+                    awc_plan** out) {
+  if (!ctx || !out) return set_err(nullptr, AWC_ERR_INVALID, "ctx/out is NULL");
+  *out = nullptr;
+  return forward_impl(ctx, p, vel, coeffs, possrcs, dt2srctf, posrecs, out);
+}
+
+void awc_plan_destroy(awc_plan* plan) {
+  if (!plan) return;
+  cudaSetDevice(plan->ctx->device);
+  cudaStreamSynchronize(plan->ctx->stream);
+  delete plan;
+}
+
+int awc_plan_reset(awc_plan* P) {
+  if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
+  awc_ctx* C = P->ctx;
+  const awc_problem* p = &P->p;
+  cudaStream_t st = C->stream;
+  CUDA_TRY(&C->err, cudaSetDevice(C->device));
+  for (int b = 0; b < 3; ++b)
+    CUDA_TRY(&C->err, cudaMemsetAsync(P->buf[b], 0, P->N * P->esz, st));
+  for (int a = 0; a < p->ndim; ++a)
+    for (int s = 0; s < 2; ++s) {
+      const int64_t cs = cross_section(p, a);
+      for (int par = 0; par < 2; ++par)
+        CUDA_TRY(&C->err, cudaMemsetAsync(P->psi[a][s][par], 0, (p->halo + 1) * cs * P->esz, st));
+      if (p->halo > 0)
+        CUDA_TRY(&C->err, cudaMemsetAsync(P->xi[a][s], 0, p->halo * cs * P->esz, st));
+    }
+  if (p->nt * p->nrec > 0)
+    CUDA_TRY(&C->err, cudaMemsetAsync(P->traces, 0, p->nt * p->nrec * P->esz, st));
+  P->step = 0;
+  return AWC_OK;
+}
+
+int awc_plan_run(awc_plan* P, int64_t nsteps, int32_t use_graph, float* ms) {
+  if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
+  awc_ctx* C = P->ctx;
+  if (nsteps < 0) return set_err(&C->err, AWC_ERR_INVALID, "nsteps < 0");
+  CUDA_TRY(&C->err, cudaSetDevice(C->device));
+  const int64_t n = std::min<int64_t>(nsteps, P->p.nt - P->step);
+  if (ms) *ms = 0.f;
+  if (n <= 0) return AWC_OK;
+  int rc;
+  cudaGraphExec_t ex = nullptr;
+  if (use_graph && (rc = get_graph(P, P->step, n, &ex))) return rc;
+  CUDA_TRY(&C->err, cudaEventRecord(C->ev0, C->stream));
+  if (use_graph) {
+    CUDA_TRY(&C->err, cudaGraphLaunch(ex, C->stream));
+  } else if ((rc = launch_range(P, P->step, n, C->stream))) {
+    return rc;
+  }
+  CUDA_TRY(&C->err, cudaEventRecord(C->ev1, C->stream));
+  CUDA_TRY(&C->err, cudaEventSynchronize(C->ev1));
+  if (ms) CUDA_TRY(&C->err, cudaEventElapsedTime(ms, C->ev0, C->ev1));
+  P->step += n;
+  return AWC_OK;
+}
+
+int64_t awc_plan_step(const awc_plan* P) { return P ? P->step : -1; }
+
+int awc_plan_traces(awc_plan* P, double* traces) {
+  if (!P || !traces) return set_err(nullptr, AWC_ERR_INVALID, "plan/traces is NULL");
+  awc_ctx* C = P->ctx;
+  const int64_t nt = P->p.nt, nrec = P->p.nrec;
+  if (nt * nrec == 0) return AWC_OK;
+  CUDA_TRY(&C->err, cudaSetDevice(C->device));
+  dim3 grid((unsigned)((nt + 31) / 32), (unsigned)((nrec + 31) / 32));
+  if (P->p.precision == AWC_F64)
+    awc::traces_out<double><<<grid, dim3(32, 8), 0, C->stream>>>((const double*)P->traces, P->staging, nt, nrec);
+  else
+    awc::traces_out<float><<<grid, dim3(32, 8), 0, C->stream>>>((const float*)P->traces, P->staging, nt, nrec);
+  CUDA_TRY(&C->err, cudaGetLastError());
+  CUDA_TRY(&C->err, cudaMemcpyAsync(traces, P->staging, nt * nrec * 8, cudaMemcpyDeviceToHost, C->stream));
+  CUDA_TRY(&C->err, cudaStreamSynchronize(C->stream));
+  return AWC_OK;
+}
+
+int awc_plan_field(awc_plan* P, double* out) {
+  if (!P || !out) return set_err(nullptr, AWC_ERR_INVALID, "plan/out is NULL");
+  awc_ctx* C = P->ctx;
+  CUDA_TRY(&C->err, cudaSetDevice(C->device));
+  // after s steps the latest new field is buf[(s+1)%3] (the reference's pcur)
+  const void* cur = P->buf[(P->step + 1) % 3];
+  if (P->p.precision == AWC_F64) {
+    CUDA_TRY(&C->err, cudaMemcpyAsync(out, cur, P->N * 8, cudaMemcpyDeviceToHost, C->stream));
+  } else {
+    const int blocks = (int)std::min<int64_t>((P->N + 255) / 256, (int64_t)C->num_sms * 16);
+    awc::widen<float><<<blocks, 256, 0, C->stream>>>((const float*)cur, P->staging, P->N);
+    CUDA_TRY(&C->err, cudaGetLastError());
+    CUDA_TRY(&C->err, cudaMemcpyAsync(out, P->staging, P->N * 8, cudaMemcpyDeviceToHost, C->stream));
+  }
+  CUDA_TRY(&C->err, cudaStreamSynchronize(C->stream));
+  return AWC_OK;
+}
+
+int32_t awc_plan_launches_per_step(const awc_plan* P) {
+  if (!P) return 0;
+  return 1 + ((P->p.nsrc > 0 || P->p.nrec > 0) ? 1 : 0);
+}
+
+int awc_forward(awc_ctx* ctx, const awc_problem* p, const double* vel, const double* coeffs,
+                const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
+                double* traces, double* pfinal) {
+  if (!ctx) return set_err(nullptr, AWC_ERR_INVALID, "ctx is NULL");
+  int rc = validate(p, &ctx->err);
+  if (rc) return rc;
+  if (p->nt * p->nrec > 0 && !traces) return set_err(&ctx->err, AWC_ERR_INVALID, "traces is NULL");
+  // reuse a cached plan of the same shape: same buffers, same graphs
+  awc_plan* P = nullptr;
+  for (size_t c = 0; c < ctx->cache.size(); ++c)
+    if (same_shape(ctx->cache[c]->p, *p)) {
+      P = ctx->cache[c];
+      ctx->cache.erase(ctx->cache.begin() + c);
+      break;
+    }
+  if (P) {
+    if ((rc = check_positions(p, possrcs, p->nsrc, "source", &ctx->err)) ||
+        (rc = check_positions(p, posrecs, p->nrec, "receiver", &ctx->err))) {
+      ctx->cache.push_back(P);
+      return rc;
+    }
+    if (!vel || !coeffs || (p->nsrc > 0 && p->nt > 0 && !dt2srctf)) {
+      ctx->cache.push_back(P);
+      return set_err(&ctx->err, AWC_ERR_INVALID, "vel/coeffs/dt2srctf is NULL");
+    }
+    P->p = *p;
+    if (p->ndim == 2) P->p.nz = 1;
+    if ((rc = plan_upload(P, vel, coeffs, possrcs, dt2srctf, posrecs)) || (rc = awc_plan_reset(P))) {
+      delete P;
+      return rc;
+    }
+  } else {
+    if ((rc = forward_impl(ctx, p, vel, coeffs, possrcs, dt2srctf, posrecs, &P))) return rc;
+  }
+  ctx->cache.push_back(P);
+  while (ctx->cache.size() > 2) {
+    delete ctx->cache.front();
+    ctx->cache.erase(ctx->cache.begin());
+  }
+  if ((rc = awc_plan_run(P, p->nt, 1, &ctx->last_run_ms))) return rc;
+  if (traces && (rc = awc_plan_traces(P, traces))) return rc;
+  if (pfinal && (rc = awc_plan_field(P, pfinal))) return rc;
+  return AWC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,77 @@
+"""Seeded synthetic workloads with the shapes of the benchmark configurations.
+
+Grid conventions: a CPML axis has interior + 2*halo nodes; the depth axis
+(j, the reference's second axis) with a free top has interior + halo nodes,
+node j = 1 being the Dirichlet surface. Positions are given in metres as
+(node - 1) * d, so they snap back exactly to the intended 1-based node.
+Each builder returns a dict with the solve2D/solve3D arguments:
+lengths, lt, vel, srcs (positions, t0s, f0), recs (positions), kwargs.
+"""
+import math
+
+import numpy as np
+
+
+def gaussian_smooth(a, sigma):
+    """Gaussian filter (reflecting edges, truncated at 3 sigma)."""
+    from scipy.ndimage import gaussian_filter
+
+    return gaussian_filter(a, sigma=sigma, mode="reflect", truncate=3.0)
+
+
+def config1():
+    """2D FP64, the reference's CPU-runnable size: 201^2 interior + CPML 20
+    (241 x 241 nodes), dx = dy = 10 m, c = 2000 m/s, R = 1e-3, no free top,
+    Ricker f0 = 8 Hz, t0 = 0.5 s at the centre node (121, 121),
+    dt = 0.7 dx / (c sqrt 2), nt = 1000, 21 receivers on row j = 31 (10 nodes
+    below the top of the interior), i = 21, 31, ..., 221."""
+    n, dx, c = 241, 10.0, 2000.0
+    L = (n - 1) * dx
+    f0 = 8.0
+    dt = 0.7 * dx / (c * math.sqrt(2.0))
+    recs = [[(i - 1) * dx, 30 * dx] for i in range(21, 222, 10)]
+    return dict(name="cpml2d_241x241_f64_nt1000", lengths=(L, L), lt=None,
+                vel=np.full((n, n), c, order="F"), src_pos=[[120 * dx, 120 * dx]], t0s=[0.5],
+                f0=f0, rec_pos=recs, kwargs=dict(halo=20, rcoef=1e-3, freetop=False, dt=dt,
+                                                 nt=1000))
+
+
+def config2_model(seed=1234, interior=256, halo=20, dx=10.0):
+    """c(depth) = 1500 + 1.5 depth_m times (1 + 5% seeded Gaussian-smoothed
+    noise, sigma = 8 nodes), on (interior + 2 halo, interior + halo,
+    interior + 2 halo) nodes, depth on the second axis."""
+    nx = nz = interior + 2 * halo
+    ny = interior + halo
+    base = 1500.0 + 1.5 * (np.arange(ny, dtype=np.float64) * dx)
+    rng = np.random.default_rng(seed)
+    noise = gaussian_smooth(rng.standard_normal((nx, ny, nz), dtype=np.float64), 8.0)
+    noise *= 0.05 / np.abs(noise).max()
+    return np.asfortranarray(base[None, :, None] * (1.0 + noise))
+
+
+def config2(nt=2000, seed=1234, interior=256):
+    """3D single shot, the headline benchmark: 256^3 interior (296 x 276 x 296
+    nodes), dx = 10 m, model of config2_model, halo 20, free top, Ricker
+    f0 = 10 Hz at interior (128, 128, 10) = node (148, 11, 148),
+    dt = 0.6 dx / (cmax sqrt 3), nt = 2000, 64 x 64 receivers on depth node
+    j = 6 at i, k = 23, 27, ..., 275."""
+    dx, halo = 10.0, 20
+    vel = config2_model(seed=seed, interior=interior, halo=halo, dx=dx)
+    nx, ny, nz = vel.shape
+    f0 = 10.0
+    dt = 0.6 * dx / (float(vel.max()) * math.sqrt(3.0))
+    c = interior // 2
+    src = [[(c + halo - 1) * dx, 10 * dx, (c + halo - 1) * dx]]
+    idx = [i for i in (21 + 4 * a + 2 for a in range(64)) if i <= nx - 1]
+    recs = [[(i - 1) * dx, 5 * dx, (k - 1) * dx] for k in idx for i in idx]
+    L = ((nx - 1) * dx, (ny - 1) * dx, (nz - 1) * dx)
+    return dict(name=f"cpml3d_{nx}x{ny}x{nz}_freetop_nt{nt}", lengths=L, lt=None, vel=vel,
+                src_pos=src, t0s=[4 / f0], f0=f0, rec_pos=recs,
+                kwargs=dict(halo=halo, rcoef=1e-4, freetop=True, dt=dt, nt=nt))
+
+
+def sources_receivers(pkg, w):
+    """Sources/Receivers objects (Ricker source functions) of a workload."""
+    srcs = pkg.Sources(w["src_pos"], w["t0s"], [pkg.rickersource1D] * len(w["t0s"]), w["f0"])
+    recs = pkg.Receivers(w["rec_pos"])
+    return srcs, recs

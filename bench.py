@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the CPML forward time stepping on B200.
+
+Workload (default): the 3D single-shot case of the headline metric —
+256^3 interior + CPML 20 with a free top (296 x 276 x 296 nodes), seeded
+smoothed-gradient velocity model, FP32 build, nt = 2000 time steps, 4096
+receivers. One benchmark "step" is one shot: state reset + nt time steps.
+
+Metric: T_eff = A_eff / t_timestep in GB/s, with A_eff the reference's
+effective-access count (src/shared/acoustic_3D_xPU.jl:520-528) in words of
+the computed precision. `value` is measured on device-resident inputs;
+`e2e` goes through awc_forward (the drop-in C ABI call) from pinned host
+buffers, copies included. Run under torchrun for N GPUs: every rank runs its
+own shot (weak scaling, no data-path collective); timing is the max over
+ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import datetime
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import __graft_entry__ as G  # noqa: E402
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nt", type=int, default=2000, help="time steps per shot")
+    ap.add_argument("--interior", type=int, default=256, help="interior nodes per axis")
+    ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
+    ap.add_argument("--quick", action="store_true",
+                    help="device-resident leg only (no e2e, FP64 or CPU legs); for profiling")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target CPU time of the CPU-baseline sample")
+    return ap.parse_args()
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def ncu_traffic(kernel_tag):
+    """Per-launch DRAM bytes of the step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", f"ncu_{kernel_tag}.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id):
+        self.bus_id = bus_id
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        import tempfile
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms",
+               "100"]
+        if self.bus_id:
+            cmd += ["-i", self.bus_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[c - 5] for r in rows for c in range(5, 9)
+                          if r[c].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def bus_id_of(dev):
+    import torch
+    try:
+        pr = torch.cuda.get_device_properties(dev)
+        return f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+    except Exception:
+        return None
+
+
+def workload(args):
+    pkg = G.load_package()
+    from acousticwavecpml_b200 import workloads as W
+    w = W.config2(nt=args.nt, interior=args.interior)
+    srcs, recs = W.sources_receivers(pkg, w)
+    return pkg, w, srcs, recs
+
+
+def cpu_baseline(w, seconds):
+    """The oracle (C++ FP64 OpenMP restatement of the reference's Threads
+    path) on a bounded sample of the same shot: the first n time steps."""
+    O = G.load_oracle()
+    kw = dict(w["kwargs"])
+    s = O.setup(w["lengths"], w["lt"], w["vel"], w["src_pos"], w["t0s"], w["f0"], w["rec_pos"],
+                **kw)
+    p = s["problem"]
+    O.forward(s, steps=2)
+    per = O.last_loop_seconds() / 2
+    n = int(max(3, min(p.nt, seconds / max(per, 1e-6))))
+    O.forward(s, steps=n)
+    t = O.last_loop_seconds()
+    return s, n, t, O.max_threads()
+
+
+def a_eff(pkg, problem):
+    from acousticwavecpml_b200.core import a_eff_words, word_bytes
+    return a_eff_words(problem) * word_bytes(problem)
+
+
+def interior_cells(p):
+    return (p.nx - 2) * (p.ny - 2) * ((p.nz - 2) if p.ndim == 3 else 1)
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path, restated (Julia is not
+    available), FP64 on all host cores; each step is a bounded sample."""
+    pkg, w, srcs, recs = workload(args)
+    O = G.load_oracle()
+    s = O.setup(w["lengths"], w["lt"], w["vel"], w["src_pos"], w["t0s"], w["f0"], w["rec_pos"],
+                **w["kwargs"])
+    p = s["problem"]
+    O.forward(s, steps=2)
+    per = O.last_loop_seconds() / 2
+    n = int(max(2, min(p.nt, 8.0 / max(per, 1e-6))))  # ~8 s per step
+    for _ in range(args.warmup):
+        O.forward(s, steps=min(n, 2))
+    tot = 0.0
+    for _ in range(args.steps):
+        O.forward(s, steps=n)
+        tot += O.last_loop_seconds()
+    t_step = tot / (args.steps * n)
+    ab = a_eff(pkg, p)
+    val = ab / t_step / 1e9
+    line = {
+        "impl": "reference", "metric": "3D T_eff GB/s vs HBM peak", "value": val, "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded smoothed-gradient model)",
+        "config": {"workload": w["name"], "grid": [p.nx, p.ny, p.nz], "nt": p.nt,
+                   "halo": p.halo, "freetop": True,
+                   "sample": f"first {n} of {p.nt} time steps per step"},
+        "gcells_per_s": interior_cells(p) / t_step / 1e9,
+        "cpu_baseline": {"value": val, "unit": "GB/s", "cores": O.max_threads(), "kind": "port",
+                         "sample": f"{n} time steps of {w['name']} per step, FP64, "
+                                   "C++/OpenMP restatement of the Threads path"},
+        "e2e": {"value": val, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    pkg, w, srcs, recs = workload(args)
+    s = pkg.prepare(w["lengths"], w["lt"], w["vel"], srcs, recs, precision=args.precision,
+                    **w["kwargs"])
+    p = s["problem"]
+    nt = p.nt
+    ctx = pkg.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+
+    def timed(fn, k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # ---- device-resident leg ------------------------------------------------
+    plan = ctx.plan(p, s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"], s["posrecs"])
+
+    def shot():
+        plan.reset()
+        plan.run(nt, graph=True)
+
+    for _ in range(max(args.warmup, 0)):
+        shot()
+    with ClockSampler(bus_id_of(local)) as clk:
+        ms = timed(shot, args.steps)
+    clocks = clk.summary()
+    traces_dev = plan.traces()
+    launches = args.steps * nt * plan.launches_per_step
+    plan.close()
+
+    ab = a_eff(pkg, p)
+    t_ts = ms / 1e3 / (args.steps * nt)  # seconds per time step (this rank's max)
+    value = world * ab / t_ts / 1e9
+    peak, peak_src = measured_peak()
+    tag = f"step3d_{args.precision}_{p.nx}x{p.ny}x{p.nz}"
+    traffic = ncu_traffic(tag)
+    achieved = ab / t_ts / 1e9
+    line = {
+        "metric": "3D T_eff GB/s vs HBM peak", "value": value, "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.precision,
+        "data": "synthetic (seeded smoothed-gradient velocity model, Ricker source)",
+        "config": {"workload": w["name"], "grid": [p.nx, p.ny, p.nz], "nt": nt, "halo": p.halo,
+                   "freetop": True, "nrec": p.nrec, "precision": args.precision,
+                   "step": "one shot = state reset + nt fused time steps (CUDA graph)",
+                   "l2": "inputs larger than L2 (4 fields of "
+                         f"{p.nx * p.ny * p.nz * (4 if args.precision == 'f32' else 8) / 1e6:.1f}"
+                         " MB each, no flush needed)",
+                   "parallelism": f"shots{world}"},
+        "gcells_per_s": world * interior_cells(p) / t_ts / 1e9,
+        "us_per_timestep": t_ts * 1e6,
+        "a_eff_bytes_per_timestep": ab,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_src,
+                     "per_launch": "one time step (step kernel + source/receiver kernel), "
+                                   "CUDA-event time of the graph replay / launches"},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+
+    if not args.quick:
+        # ---- end-to-end through the C ABI from pinned host buffers ----------
+        vel_h = torch.empty(s["vel"].size, dtype=torch.float64, pin_memory=True)
+        vel_h.numpy()[:] = s["vel"].ravel(order="F")
+        tr_h = torch.empty(nt * p.nrec, dtype=torch.float64, pin_memory=True)
+        pf_h = torch.empty(s["vel"].size, dtype=torch.float64, pin_memory=True)
+
+        def e2e_call():
+            ctx.forward(p, vel_h, s["coeffs"], s["possrcs"], s["dt2srctf"], s["posrecs"], tr_h,
+                        pf_h)
+
+        for _ in range(max(args.warmup, 1)):
+            e2e_call()
+        ms_e2e = timed(e2e_call, args.steps)
+        tr_e2e = tr_h.numpy().reshape((nt, p.nrec), order="F")
+        h2d = (s["vel"].nbytes + s["coeffs"].nbytes + s["possrcs"].nbytes + s["dt2srctf"].nbytes +
+               s["posrecs"].nbytes)
+        d2h = tr_h.numel() * 8 + pf_h.numel() * 8
+        line["e2e"] = {"value": world * ab * nt / (ms_e2e / 1e3 / args.steps) / 1e9,
+                       "unit": "GB/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                       "ms_per_step": ms_e2e / args.steps,
+                       "call": "awc_forward (host buffers, pinned)"}
+        line["e2e_matches_device_leg"] = bool(np.array_equal(tr_e2e, traces_dev))
+
+        # ---- FP64 build of the same shot (parity build), device-resident ----
+        if args.precision == "f32":
+            s64 = pkg.prepare(w["lengths"], w["lt"], w["vel"], srcs, recs, precision="f64",
+                              **w["kwargs"])
+            p64 = s64["problem"]
+            plan64 = ctx.plan(p64, s64["vel"], s64["coeffs"], s64["possrcs"], s64["dt2srctf"],
+                              s64["posrecs"])
+
+            def shot64():
+                plan64.reset()
+                plan64.run(nt, graph=True)
+
+            shot64()
+            k64 = max(1, min(args.steps, 3))
+            ms64 = timed(shot64, k64)
+            tr64 = plan64.traces()
+            plan64.close()
+            t64 = ms64 / 1e3 / (k64 * nt)
+            ab64 = a_eff(pkg, p64)
+            line["fp64"] = {"value": world * ab64 / t64 / 1e9, "unit": "GB/s",
+                            "gcells_per_s": world * interior_cells(p64) / t64 / 1e9,
+                            "us_per_timestep": t64 * 1e6, "frac": ab64 / t64 / 1e9 / peak}
+            nrm = np.linalg.norm(tr64)
+            line["fp32_vs_fp64_traces_rel_l2"] = float(np.linalg.norm(traces_dev - tr64) /
+                                                       (nrm if nrm > 0 else 1.0))
+
+        # ---- CPU baseline (rank 0 at N=1 only) ------------------------------
+        if world == 1 and rank == 0:
+            so, n, t, cores = cpu_baseline(w, args.cpu_seconds)
+            t_cpu = t / n
+            ab_cpu = a_eff(pkg, so["problem"])
+            line["cpu_baseline"] = {
+                "value": ab_cpu / t_cpu / 1e9, "unit": "GB/s", "cores": cores, "kind": "port",
+                "sample": f"first {n} of {nt} time steps of {w['name']}, FP64, C++/OpenMP "
+                          "restatement of the reference Threads path (Julia absent)",
+                "gcells_per_s": interior_cells(so["problem"]) / t_cpu / 1e9,
+                "s_per_timestep": t_cpu}
+
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

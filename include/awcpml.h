@@ -1,0 +1,148 @@
+/*
+ * awcpml.h — C ABI of the B200 (sm_100a) CPML acoustic time-stepping library.
+ *
+ * This library replaces the device time loop behind the Julia entry points
+ * Acoustic2D_CUDA.solve2D / Acoustic3D_CUDA.solve3D of AcousticWaveCPML.jl
+ * (src/Acoustic2D_CUDA.jl:52-56, src/Acoustic3D_CUDA.jl:60-64, whose bodies are
+ * src/shared/acoustic_2D_xPU.jl:133-445 and src/shared/acoustic_3D_xPU.jl:169-545).
+ * The Julia side keeps the reference's host setup (dt, nt, CPML coefficients,
+ * source time functions, position snapping) and hands the arrays to
+ * awc_forward(); everything the reference runs through ParallelStencil kernels
+ * (update_ψ_*!, update_p!, inject_sources!, record_receivers!, forward!) runs
+ * here as one fused CUDA kernel per time step, replayed from a CUDA graph.
+ *
+ * Conventions shared by every entry point:
+ *  - Arrays are host memory, column-major (Julia layout), unless stated.
+ *  - Grid sizes nx, ny, nz count every node, CPML band and the Dirichlet rim
+ *    included (the size of `vel` in the reference). 2D problems use nz = 1.
+ *  - Positions are 1-based Int64 grid indices, (n × ndim) column-major, i.e.
+ *    pos[s + n*d] is coordinate d of item s, exactly as the reference stores
+ *    possrcs/posrecs (acoustic_3D_xPU.jl:277-289).
+ *  - Return value: AWC_OK (0) or a negative AWC_ERR_* code; the message is
+ *    available from awc_last_error(). The library never aborts the process.
+ *  - Depth is the second array axis (j, "y"), as in the reference: the free
+ *    top surface is j = 1 (acoustic_3D_xPU.jl:225-230).
+ */
+#ifndef AWCPML_H
+#define AWCPML_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AWC_OK 0
+#define AWC_ERR_INVALID (-1)  /* bad argument (shape, position, size, pointer) */
+#define AWC_ERR_OOM (-2)      /* device memory allocation failed */
+#define AWC_ERR_CUDA (-3)     /* a CUDA runtime call failed */
+#define AWC_ERR_TIMEOUT (-4)  /* a bounded device wait ran out */
+#define AWC_ERR_NODEVICE (-5) /* no usable sm_100 device */
+
+#define AWC_F32 1 /* fields, ψ, ξ and coefficients stored and updated in float */
+#define AWC_F64 2 /* everything in double (parity build) */
+
+/* One forward problem: a single shot on one velocity model.
+ * Mirrors the scalars solve2D/solve3D derive (acoustic_3D_xPU.jl:195-206). */
+typedef struct awc_problem {
+  int32_t ndim;      /* 2 or 3 */
+  int32_t precision; /* AWC_F32 or AWC_F64 */
+  int64_t nx, ny, nz;
+  int32_t halo;    /* CPML layers per side (reference keyword `halo`) */
+  int32_t freetop; /* 1: no CPML on the j = 1 side (coefficients say so too) */
+  double dx, dy, dz; /* grid spacing [m]; dz ignored in 2D */
+  double dt;         /* time step [s] */
+  int64_t nt;        /* number of time steps */
+  int64_t nsrc, nrec;
+} awc_problem;
+
+/* Number of doubles in the packed CPML coefficient array for `p`:
+ * ndim blocks of (8*halo + 4), each block laid out as
+ *   a_l[halo] a_r[halo] bK_l[halo] bK_r[halo]
+ *   a_hl[halo+1] a_hr[halo+1] bK_hl[halo+1] bK_hr[halo+1]
+ * for axis x, then y, then z (the 24 vectors of acoustic_3D_xPU.jl:218-223). */
+int64_t awc_coeffs_len(const awc_problem* p);
+
+/* calc_Kab_CPML (src/utils.jl:19-57): K, a, b CPML profile of `halo` layers.
+ * halfgrid = 0 gives the on-grid set (length halo), 1 the staggered set
+ * (length halo+1). Outputs a_l, a_r, bK_l = b/K left, bK_r = b/K right. FP64. */
+int awc_cpml_coeffs(int32_t halo, double dt, double npower, double d0, double alpha_max,
+                    double K_max, int32_t halfgrid, double* a_l, double* a_r, double* bK_l,
+                    double* bK_r);
+
+/* The CPML block of solve2D/solve3D (acoustic_3D_xPU.jl:207-230,
+ * acoustic_2D_xPU.jl:166-185): alpha_max = π f0, npower = 2, K_max = 1,
+ * d0 = -(npower+1) vel_max log(rcoef) / (2 halo d) per axis, both grids, then
+ * the free-top override when p->freetop. Fills awc_coeffs_len(p) doubles. */
+int awc_problem_coeffs(const awc_problem* p, double rcoef, double f0, double vel_max,
+                       double* coeffs);
+
+/* rickersource1D (src/utils.jl:64-66) evaluated at n times. */
+int awc_ricker(int64_t n, const double* t, double t0, double f0, double* out);
+
+/* Opaque per-thread context: owns the CUDA stream, device buffers and the
+ * captured time-loop graphs (cached by problem shape). Not thread-safe; use
+ * one context per host thread. */
+typedef struct awc_ctx awc_ctx;
+
+/* Creates a context on CUDA device `device` (must be sm_100). */
+int awc_create(awc_ctx** out, int32_t device);
+void awc_destroy(awc_ctx* ctx);
+/* Last error message of `ctx`, or of the calling thread when ctx is NULL. */
+const char* awc_last_error(const awc_ctx* ctx);
+/* Device time [ms] of the time loop of the last awc_forward on `ctx`
+ * (CUDA events around the graph replay; host copies excluded). */
+float awc_last_run_ms(const awc_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), on which every copy and kernel
+ * of the context is ordered; callers may record their own events on it. */
+void* awc_ctx_stream(const awc_ctx* ctx);
+
+/* The forward solve (the time loop of acoustic_3D_xPU.jl:392-409 and the
+ * returns at :541-544; 2D acoustic_2D_xPU.jl:327-343, :441-444).
+ *   vel      [nx*ny*nz]       velocity [m/s]; fact = dt^2 vel^2 is formed on
+ *                             the device in FP64 (acoustic_3D_xPU.jl:242)
+ *   coeffs   [awc_coeffs_len] packed CPML vectors (awc_problem_coeffs)
+ *   possrcs  [nsrc*ndim]      1-based source nodes
+ *   dt2srctf [nt*nsrc]        scaled source time functions, column-major
+ *                             (acoustic_3D_xPU.jl:272-275)
+ *   posrecs  [nrec*ndim]      1-based receiver nodes
+ *   traces   [nt*nrec] out    recorded pressure, traces[it + nt*r]
+ *   pfinal   [nx*ny*nz] out   final field (the reference's Array(pcur));
+ *                             may be NULL
+ * Step it (1-based) updates ψ, ξ and p, adds dt2srctf[it, s] into the new
+ * field at each source, then records the new field at each receiver. Several
+ * sources on one node are summed in source order. */
+int awc_forward(awc_ctx* ctx, const awc_problem* p, const double* vel, const double* coeffs,
+                const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
+                double* traces, double* pfinal);
+
+/* Device-resident plan: the inputs of awc_forward uploaded once, the state
+ * kept in HBM between calls. awc_forward is plan create + run(nt) + read-out.
+ * The plan belongs to its context and must be destroyed before it. */
+typedef struct awc_plan awc_plan;
+
+int awc_plan_create(awc_ctx* ctx, const awc_problem* p, const double* vel, const double* coeffs,
+                    const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
+                    awc_plan** out);
+void awc_plan_destroy(awc_plan* plan);
+/* Zeroes pressure, ψ, ξ and traces; the next run starts at it = 1. */
+int awc_plan_reset(awc_plan* plan);
+/* Advances `nsteps` time steps (clamped to nt). use_graph = 1 replays a
+ * captured CUDA graph, 0 launches the kernels one by one. When ms != NULL the
+ * device time of the run, measured with CUDA events on the plan's stream, is
+ * written there. Returns after the run completes. */
+int awc_plan_run(awc_plan* plan, int64_t nsteps, int32_t use_graph, float* ms);
+/* Steps completed since the last reset. */
+int64_t awc_plan_step(const awc_plan* plan);
+/* Copies the traces (nt*nrec, column-major; rows not yet reached are zero)
+ * and the current field (the latest new pressure, nx*ny*nz) to the host. */
+int awc_plan_traces(awc_plan* plan, double* traces);
+int awc_plan_field(awc_plan* plan, double* p);
+/* Number of kernel launches one time step issues (for launch accounting). */
+int32_t awc_plan_launches_per_step(const awc_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AWCPML_H */
