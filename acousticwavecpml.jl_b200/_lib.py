@@ -78,6 +78,7 @@ SIGNATURES = {
     "awc_last_error": (ctypes.c_char_p, [_vp]),
     "awc_last_run_ms": (ctypes.c_float, [_vp]),
     "awc_ctx_stream": (ctypes.c_void_p, [_vp]),
+    "awc_ctx_set_autotune": (ctypes.c_int, [_vp, ctypes.c_int64]),
     "awc_forward": (ctypes.c_int, [_vp, _PP, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "awc_plan_create": (ctypes.c_int, [_vp, _PP, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_vp)]),
     "awc_plan_destroy": (None, [_vp]),
@@ -88,6 +89,12 @@ SIGNATURES = {
     "awc_plan_traces": (ctypes.c_int, [_vp, _vp]),
     "awc_plan_field": (ctypes.c_int, [_vp, _vp]),
     "awc_plan_launches_per_step": (ctypes.c_int32, [_vp]),
+    "awc_plan_set_launch": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32,
+                                           ctypes.c_int32]),
+    "awc_plan_get_launch": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32)]),
+    "awc_plan_autotune": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_float)]),
 }
 
 _LIB = None

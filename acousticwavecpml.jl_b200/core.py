@@ -59,6 +59,11 @@ class Context:
         """The context's cudaStream_t as an integer handle."""
         return int(_lib.lib().awc_ctx_stream(self._h) or 0)
 
+    def set_autotune(self, steps):
+        """Steps per candidate of the launch-shape autotuning that forward()
+        runs for each new 3D problem shape (0 disables it)."""
+        check(_lib.lib().awc_ctx_set_autotune(self._h, int(steps)), self._h)
+
     def forward(self, problem, vel, coeffs, possrcs, dt2srctf, posrecs, traces, pfinal=None):
         """awc_forward on host buffers (numpy arrays or pinned torch tensors)."""
         rc = _lib.lib().awc_forward(self._h, ctypes.byref(problem), _ptr(vel), _ptr(coeffs),
@@ -127,6 +132,25 @@ class Plan:
     @property
     def launches_per_step(self):
         return int(_lib.lib().awc_plan_launches_per_step(self._h))
+
+    def set_launch(self, kernel, tile_y, zchunk):
+        """3D launch shape: kernel 0 (register queue) or 1 (TMA pipeline)."""
+        check(_lib.lib().awc_plan_set_launch(self._h, int(kernel), int(tile_y), int(zchunk)),
+              self.ctx.handle)
+
+    def get_launch(self):
+        kn, ty, zc = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(_lib.lib().awc_plan_get_launch(self._h, ctypes.byref(kn), ctypes.byref(ty),
+                                             ctypes.byref(zc)), self.ctx.handle)
+        return kn.value, ty.value, zc.value
+
+    def autotune(self, steps=20):
+        """Picks the fastest launch shape on this plan's data; resets the state.
+        Returns the best time per step in ms."""
+        ms = ctypes.c_float(0.0)
+        check(_lib.lib().awc_plan_autotune(self._h, int(steps), ctypes.byref(ms)),
+              self.ctx.handle)
+        return float(ms.value)
 
     def traces(self, out=None):
         p = self.problem

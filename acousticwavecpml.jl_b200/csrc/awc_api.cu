@@ -4,7 +4,10 @@
 // (positions inside the model, src/shared/acoustic_3D_xPU.jl:281,289; halo
 // small enough for the band index arithmetic of :12,:68), the FP64 CPML
 // coefficient setup (src/utils.jl:19-57), device buffers, the per-step launch
-// sequence of forward! (:124-167) and its capture into CUDA graphs.
+// sequence of forward! (:124-167), its capture into CUDA graphs, and the
+// launch-shape autotuner.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -13,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <unordered_map>
 #include <utility>
@@ -125,10 +129,33 @@ int check_positions(const awc_problem* p, const int64_t* pos, int64_t cnt, const
   return AWC_OK;
 }
 
-int64_t node_of(const awc_problem* p, const int64_t* pos, int64_t cnt, int64_t s) {
+// Row pitch of the field arrays: nx rounded up to 32 elements.
+int64_t pitch_of(int64_t nx) { return (nx + 31) / 32 * 32; }
+
+// Pitched linear index of item s of a 1-based (cnt x ndim) position array.
+int64_t node_of(const awc_problem* p, int64_t px, const int64_t* pos, int64_t cnt, int64_t s) {
   const int64_t i = pos[s] - 1, j = pos[s + cnt] - 1, k = p->ndim == 3 ? pos[s + 2 * cnt] - 1 : 0;
-  return i + p->nx * (j + p->ny * k);
+  return i + px * (j + p->ny * k);
 }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+constexpr int kTmaStages = 6;  // pipeline depth of step3d_tma (3 planes ahead)
 
 }  // namespace
 
@@ -139,6 +166,7 @@ struct awc_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;
   float last_run_ms = 0.f;
+  int64_t autotune_steps = 10;   // per candidate, for new 3D plans of awc_forward
   std::vector<awc_plan*> cache;  // plans reused by awc_forward, most recent last
 };
 
@@ -146,27 +174,42 @@ struct awc_plan {
   awc_ctx* ctx = nullptr;
   awc_problem p{};
   size_t esz = 0;  // bytes per element of T
-  int64_t N = 0;   // nodes
+  int64_t N = 0;   // nodes (dense count)
+  int64_t px = 0;  // field row pitch (elements)
+  int64_t NP = 0;  // pitched field length
   // device buffers
   void* buf[3] = {nullptr, nullptr, nullptr};
   void* fact = nullptr;
   void* psi[3][2][2] = {};  // [axis][side][old/new parity]
   void* xi[3][2] = {};
   void* coef = nullptr;  // packed coefficients in T
-  int64_t* src_node = nullptr;
+  int32_t* err_flag = nullptr;
+  // sources and receivers: groups per node (CSR), the nodes themselves, and
+  // their layout for the current launch shape (see awc::Io)
   int32_t* src_off = nullptr;
   int32_t* src_ids = nullptr;
-  int32_t nsrc_nodes = 0;
-  void* stf = nullptr;  // [nt][nsrc]
-  int64_t* rec_node = nullptr;
+  int32_t* rec_off = nullptr;
+  int32_t* rec_ids = nullptr;
+  std::vector<awc::IoRim> io_nodes;  // host copy: node, source group, receiver group
+  int32_t* io_blk_off = nullptr;
+  int64_t io_blk_cap = 0;
+  int4* io_ent = nullptr;
+  awc::IoRim* io_rim = nullptr;
+  int32_t io_nrim = 0;
+  uint64_t io_shape = ~0ull;  // launch shape io_* were built for
+  uint32_t io_version = 0;
+  void* stf = nullptr;     // [nt][nsrc]
   void* traces = nullptr;  // [nt][nrec]
   double* staging = nullptr;
   int64_t staging_len = 0;
   std::vector<void*> allocs;
+  // launch shape: kernel 0 = register queue, 1 = TMA pipeline (3D)
+  int32_t kernel = 0, by = 8, zchunk = 1;
+  CUtensorMap map_c[3], map_o[3], map_f;
+  int32_t maps_by = 0;  // tile height the tensor maps were encoded for
   // run state
   int64_t step = 0;
   int32_t active[3][2] = {};
-  int32_t by = 8, zchunk = 0;
   std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
   uint64_t graph_key = 0;  // launch configuration the graphs were captured with
 
@@ -181,6 +224,12 @@ struct awc_plan {
     }
     allocs.push_back(*out);
     return AWC_OK;
+  }
+  void release(void* ptr) {
+    if (!ptr) return;
+    auto f = std::find(allocs.begin(), allocs.end(), ptr);
+    if (f != allocs.end()) allocs.erase(f);
+    cudaFree(ptr);
   }
   void drop_graphs() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -204,11 +253,14 @@ int plan_alloc(awc_plan* P) {
   const awc_problem* p = &P->p;
   const int64_t h = p->halo;
   P->esz = p->precision == AWC_F64 ? 8 : 4;
-  P->N = p->nx * p->ny * (p->ndim == 3 ? p->nz : 1);
+  const int64_t nz = p->ndim == 3 ? p->nz : 1;
+  P->N = p->nx * p->ny * nz;
+  P->px = pitch_of(p->nx);
+  P->NP = P->px * p->ny * nz;
   int rc;
   for (int b = 0; b < 3; ++b)
-    if ((rc = P->alloc(&P->buf[b], P->N * P->esz))) return rc;
-  if ((rc = P->alloc(&P->fact, P->N * P->esz))) return rc;
+    if ((rc = P->alloc(&P->buf[b], P->NP * P->esz))) return rc;
+  if ((rc = P->alloc(&P->fact, P->NP * P->esz))) return rc;
   for (int a = 0; a < p->ndim; ++a)
     for (int s = 0; s < 2; ++s) {
       const int64_t cs = cross_section(p, a);
@@ -217,14 +269,19 @@ int plan_alloc(awc_plan* P) {
       if ((rc = P->alloc(&P->xi[a][s], h * cs * P->esz))) return rc;
     }
   if ((rc = P->alloc(&P->coef, awc_coeffs_len(p) * P->esz))) return rc;
-  if ((rc = P->alloc((void**)&P->src_node, std::max<int64_t>(p->nsrc, 1) * 8))) return rc;
-  if ((rc = P->alloc((void**)&P->src_off, (std::max<int64_t>(p->nsrc, 1) + 1) * 4))) return rc;
-  if ((rc = P->alloc((void**)&P->src_ids, std::max<int64_t>(p->nsrc, 1) * 4))) return rc;
+  if ((rc = P->alloc((void**)&P->err_flag, 4))) return rc;
+  const int64_t ns = std::max<int64_t>(p->nsrc, 1), nr = std::max<int64_t>(p->nrec, 1);
+  if ((rc = P->alloc((void**)&P->src_off, (ns + 1) * 4))) return rc;
+  if ((rc = P->alloc((void**)&P->src_ids, ns * 4))) return rc;
+  if ((rc = P->alloc((void**)&P->rec_off, (nr + 1) * 4))) return rc;
+  if ((rc = P->alloc((void**)&P->rec_ids, nr * 4))) return rc;
+  if ((rc = P->alloc((void**)&P->io_ent, (ns + nr) * sizeof(int4)))) return rc;
+  if ((rc = P->alloc((void**)&P->io_rim, (ns + nr) * sizeof(awc::IoRim)))) return rc;
   if ((rc = P->alloc(&P->stf, std::max<int64_t>(p->nt * p->nsrc, 1) * P->esz))) return rc;
-  if ((rc = P->alloc((void**)&P->rec_node, std::max<int64_t>(p->nrec, 1) * 8))) return rc;
   if ((rc = P->alloc(&P->traces, std::max<int64_t>(p->nt * p->nrec, 1) * P->esz))) return rc;
   P->staging_len = std::max<int64_t>(P->N, p->nt * p->nrec);
   if ((rc = P->alloc((void**)&P->staging, P->staging_len * 8))) return rc;
+  CUDA_TRY(&P->ctx->err, cudaMemsetAsync(P->err_flag, 0, 4, P->ctx->stream));
   return AWC_OK;
 }
 
@@ -233,6 +290,11 @@ void to_T(const double* src, std::vector<unsigned char>& out, int64_t n) {
   out.resize(n * sizeof(T));
   T* d = reinterpret_cast<T*>(out.data());
   for (int64_t c = 0; c < n; ++c) d[c] = (T)src[c];
+}
+
+int grid_for(const awc_ctx* C, int64_t n, int threads) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads,
+                                                     (int64_t)C->num_sms * 16));
 }
 
 // Uploads the inputs of one shot into an allocated plan. The copies are
@@ -245,17 +307,17 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
   cudaStream_t st = C->stream;
   const int64_t h = p->halo, nt = p->nt, nsrc = p->nsrc, nrec = p->nrec;
   const bool f64 = p->precision == AWC_F64;
-  // fact = dt^2 vel^2 on the device in FP64
+  // fact = dt^2 vel^2 on the device in FP64, written pitched
   CUDA_TRY(err, cudaMemcpyAsync(P->staging, vel, P->N * 8, cudaMemcpyHostToDevice, st));
   {
-    const int threads = 256;
-    const int64_t want = (P->N + threads - 1) / threads;
-    const int blocks = (int)std::min<int64_t>(want, (int64_t)C->num_sms * 16);
     const double dt2 = p->dt * p->dt;
+    const int blocks = grid_for(C, P->N, 256);
     if (f64)
-      awc::make_fact<double><<<blocks, threads, 0, st>>>(P->staging, (double*)P->fact, dt2, P->N);
+      awc::make_fact<double><<<blocks, 256, 0, st>>>(P->staging, (double*)P->fact, dt2, P->N,
+                                                     p->nx, P->px);
     else
-      awc::make_fact<float><<<blocks, threads, 0, st>>>(P->staging, (float*)P->fact, dt2, P->N);
+      awc::make_fact<float><<<blocks, 256, 0, st>>>(P->staging, (float*)P->fact, dt2, P->N,
+                                                    p->nx, P->px);
     CUDA_TRY(err, cudaGetLastError());
   }
   // coefficients (and which band sides are live)
@@ -278,36 +340,56 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
       P->active[a][s] = (h > 0 && !trivial) ? 1 : 0;
     }
   }
-  // sources grouped by node in first-appearance order, summed in source order
+  // every node carrying sources and/or receivers, in first-appearance order
+  // (sources first); its sources are summed in source order
   {
-    std::vector<int64_t> nodes;
-    std::vector<std::vector<int32_t>> groups;
     std::unordered_map<int64_t, int32_t> where;
-    for (int64_t s = 0; s < nsrc; ++s) {
-      const int64_t nd = node_of(p, possrcs, nsrc, s);
-      auto it = where.find(nd);
-      if (it == where.end()) {
-        where.emplace(nd, (int32_t)nodes.size());
-        nodes.push_back(nd);
-        groups.push_back({(int32_t)s});
-      } else {
-        groups[it->second].push_back((int32_t)s);
+    std::vector<std::vector<int32_t>> sg, rg;  // groups
+    P->io_nodes.clear();
+    auto node_slot = [&](int64_t nd) -> awc::IoRim& {
+      auto f = where.find(nd);
+      if (f == where.end()) {
+        where.emplace(nd, (int32_t)P->io_nodes.size());
+        P->io_nodes.push_back(awc::IoRim{nd, -1, -1});
+        return P->io_nodes.back();
       }
+      return P->io_nodes[f->second];
+    };
+    for (int64_t s = 0; s < nsrc; ++s) {
+      awc::IoRim& e = node_slot(node_of(p, P->px, possrcs, nsrc, s));
+      if (e.sgrp < 0) {
+        e.sgrp = (int32_t)sg.size();
+        sg.emplace_back();
+      }
+      sg[e.sgrp].push_back((int32_t)s);
     }
-    std::vector<int32_t> off(1, 0), ids;
-    for (auto& g : groups) {
-      ids.insert(ids.end(), g.begin(), g.end());
-      off.push_back((int32_t)ids.size());
+    for (int64_t r = 0; r < nrec; ++r) {
+      awc::IoRim& e = node_slot(node_of(p, P->px, posrecs, nrec, r));
+      if (e.rgrp < 0) {
+        e.rgrp = (int32_t)rg.size();
+        rg.emplace_back();
+      }
+      rg[e.rgrp].push_back((int32_t)r);
     }
-    P->nsrc_nodes = (int32_t)nodes.size();
-    if (!nodes.empty()) {
-      CUDA_TRY(err, cudaMemcpyAsync(P->src_node, nodes.data(), nodes.size() * 8,
-                                    cudaMemcpyHostToDevice, st));
-      CUDA_TRY(err, cudaMemcpyAsync(P->src_ids, ids.data(), ids.size() * 4,
-                                    cudaMemcpyHostToDevice, st));
-    }
-    CUDA_TRY(err, cudaMemcpyAsync(P->src_off, off.data(), off.size() * 4,
-                                  cudaMemcpyHostToDevice, st));
+    auto csr = [](const std::vector<std::vector<int32_t>>& g, std::vector<int32_t>& off,
+                  std::vector<int32_t>& ids) {
+      off.assign(1, 0);
+      ids.clear();
+      for (auto& v : g) {
+        ids.insert(ids.end(), v.begin(), v.end());
+        off.push_back((int32_t)ids.size());
+      }
+    };
+    std::vector<int32_t> soff, sids, roff, rids;
+    csr(sg, soff, sids);
+    csr(rg, roff, rids);
+    CUDA_TRY(err, cudaMemcpyAsync(P->src_off, soff.data(), soff.size() * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(err, cudaMemcpyAsync(P->rec_off, roff.data(), roff.size() * 4, cudaMemcpyHostToDevice, st));
+    if (!sids.empty())
+      CUDA_TRY(err, cudaMemcpyAsync(P->src_ids, sids.data(), sids.size() * 4, cudaMemcpyHostToDevice, st));
+    if (!rids.empty())
+      CUDA_TRY(err, cudaMemcpyAsync(P->rec_ids, rids.data(), rids.size() * 4, cudaMemcpyHostToDevice, st));
+    P->io_shape = ~0ull;  // rebuild the block lists before the next launch
     // stf rows: [it][s] from the column-major (nt x nsrc) input
     std::vector<double> rows((size_t)std::max<int64_t>(nt * nsrc, 1), 0.0);
     for (int64_t s = 0; s < nsrc; ++s)
@@ -315,10 +397,6 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
     if (f64) to_T<double>(rows.data(), tmp, nt * nsrc); else to_T<float>(rows.data(), tmp, nt * nsrc);
     if (nt * nsrc > 0)
       CUDA_TRY(err, cudaMemcpyAsync(P->stf, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, st));
-    std::vector<int64_t> rn(std::max<int64_t>(nrec, 1));
-    for (int64_t r = 0; r < nrec; ++r) rn[r] = node_of(p, posrecs, nrec, r);
-    if (nrec > 0)
-      CUDA_TRY(err, cudaMemcpyAsync(P->rec_node, rn.data(), nrec * 8, cudaMemcpyHostToDevice, st));
     CUDA_TRY(err, cudaStreamSynchronize(st));  // host vectors go out of scope
   }
   return AWC_OK;
@@ -340,6 +418,7 @@ awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
   S.ny = (int32_t)p->ny;
   S.nz = (int32_t)(p->ndim == 3 ? p->nz : 1);
   S.halo = p->halo;
+  S.px = P->px;
   const double d[3] = {p->dx, p->dy, p->ndim == 3 ? p->dz : 1.0};
   for (int a = 0; a < 3; ++a) {
     S.inv_d[a] = (T)(1.0 / d[a]);
@@ -365,32 +444,168 @@ awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
   }
   S.zchunk = P->zchunk;
   S.it = (int32_t)it;
+  S.err = P->err_flag;
+  S.io.blk_off = P->io_blk_off;
+  S.io.ent = P->io_ent;
+  S.io.rim = P->io_rim;
+  S.io.nrim = P->io_nrim;
+  S.io.src_off = P->src_off;
+  S.io.src_ids = P->src_ids;
+  S.io.rec_off = P->rec_off;
+  S.io.rec_ids = P->rec_ids;
+  S.io.stf = (const T*)P->stf;
+  S.io.nsrc = (int32_t)p->nsrc;
+  S.io.nrec = (int32_t)p->nrec;
+  S.io.traces = (T*)P->traces;
   return S;
 }
 
-template <typename T>
-awc::Io<T> io_params(const awc_plan* P) {
-  awc::Io<T> io{};
-  io.src_node = P->src_node;
-  io.src_off = P->src_off;
-  io.src_ids = P->src_ids;
-  io.nsrc_nodes = P->nsrc_nodes;
-  io.stf = (const T*)P->stf;
-  io.nsrc = (int32_t)P->p.nsrc;
-  io.rec_node = P->rec_node;
-  io.nrec = (int32_t)P->p.nrec;
-  io.traces = (T*)P->traces;
-  return io;
+// Tile height of the current launch shape (the 2D kernel uses 8 rows).
+int tile_rows(const awc_plan* P) { return P->p.ndim == 3 ? P->by : 8; }
+
+// Launch grid of the step kernel: x tiles [32 bx, 32 bx + 32) cover nodes
+// 1..nx-2, y tiles start at node 1, z chunks at plane 1.
+dim3 step_grid(const awc_plan* P) {
+  const awc_problem* p = &P->p;
+  const unsigned gx = (unsigned)((p->nx - 2) / 32 + 1);
+  const unsigned gy = (unsigned)((p->ny - 2 + tile_rows(P) - 1) / tile_rows(P));
+  if (p->ndim == 3) return dim3(gx, gy, (unsigned)((p->nz - 2 + P->zchunk - 1) / P->zchunk));
+  return dim3(gx, gy, 1);
+}
+
+uint64_t launch_shape(const awc_plan* P) {
+  return (uint64_t)P->by | ((uint64_t)P->zchunk << 8) | ((uint64_t)P->kernel << 40);
+}
+
+// Buckets the source/receiver nodes by the block that owns them for the
+// current launch shape: rim nodes to the rim list, interior nodes to
+// (block, plane, local thread) order.
+int ensure_io(awc_plan* P) {
+  if (P->io_shape == launch_shape(P)) return AWC_OK;
+  awc_ctx* C = P->ctx;
+  const awc_problem* p = &P->p;
+  const dim3 g = step_grid(P);
+  const int64_t nblk = (int64_t)g.x * g.y * g.z;
+  const int tyh = tile_rows(P);
+  std::vector<awc::IoRim> rim;
+  std::vector<std::pair<std::pair<int64_t, int64_t>, int4>> ent;  // ((blk, k*2^32+local), entry)
+  for (const awc::IoRim& e : P->io_nodes) {
+    const int64_t i = e.node % P->px, j = (e.node / P->px) % p->ny, k = e.node / (P->px * p->ny);
+    const bool interior = i >= 1 && i <= p->nx - 2 && j >= 1 && j <= p->ny - 2 &&
+                          (p->ndim == 2 || (k >= 1 && k <= p->nz - 2));
+    if (!interior) {
+      rim.push_back(e);
+      continue;
+    }
+    const int64_t bx = i / 32, tx = i % 32, by = (j - 1) / tyh, ty = (j - 1) % tyh;
+    const int64_t bz = p->ndim == 3 ? (k - 1) / P->zchunk : 0;
+    const int64_t blk = bx + g.x * (by + (int64_t)g.y * bz);
+    const int local = (int)(tx + 32 * ty);
+    ent.push_back({{blk, (k << 32) | local}, make_int4(local, (int)k, e.sgrp, e.rgrp)});
+  }
+  std::sort(ent.begin(), ent.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+  std::vector<int32_t> off(nblk + 1, 0);
+  std::vector<int4> flat(ent.size());
+  for (size_t n = 0; n < ent.size(); ++n) {
+    off[ent[n].first.first + 1]++;
+    flat[n] = ent[n].second;
+  }
+  for (int64_t b = 0; b < nblk; ++b) off[b + 1] += off[b];
+  if (P->io_blk_cap < nblk + 1) {
+    P->release(P->io_blk_off);
+    P->io_blk_off = nullptr;
+    P->io_blk_cap = 0;
+    int rc = P->alloc((void**)&P->io_blk_off, (nblk + 1) * 4);
+    if (rc) return rc;
+    P->io_blk_cap = nblk + 1;
+  }
+  cudaStream_t st = C->stream;
+  CUDA_TRY(&C->err, cudaMemcpyAsync(P->io_blk_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st));
+  if (!flat.empty())
+    CUDA_TRY(&C->err, cudaMemcpyAsync(P->io_ent, flat.data(), flat.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  if (!rim.empty())
+    CUDA_TRY(&C->err, cudaMemcpyAsync(P->io_rim, rim.data(), rim.size() * sizeof(awc::IoRim), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(&C->err, cudaStreamSynchronize(st));
+  P->io_nrim = (int32_t)rim.size();
+  P->io_shape = launch_shape(P);
+  P->io_version++;
+  return AWC_OK;
+}
+
+// Tensor maps of the TMA variant: for each rotating field buffer a map with
+// the pcur box ((32 + 2A) x (BY + 2) x 1) and one with the pold box
+// (32 x BY x 1), and one for fact. Dims (nx, ny, nz), pitched strides.
+int ensure_maps(awc_plan* P) {
+  if (P->maps_by == P->by) return AWC_OK;
+  awc_ctx* C = P->ctx;
+  const awc_problem* p = &P->p;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return set_err(&C->err, AWC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const bool f64 = p->precision == AWC_F64;
+  const CUtensorMapDataType dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint32_t A = 16 / (cuuint32_t)P->esz;
+  const cuuint64_t dims[3] = {(cuuint64_t)p->nx, (cuuint64_t)p->ny, (cuuint64_t)p->nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)(P->px * P->esz), (cuuint64_t)(P->px * p->ny * P->esz)};
+  const cuuint32_t box_c[3] = {32 + 2 * A, (cuuint32_t)P->by + 2, 1};
+  const cuuint32_t box_i[3] = {32, (cuuint32_t)P->by, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  auto make = [&](CUtensorMap* m, void* base, const cuuint32_t* box) -> bool {
+    return enc(m, dt, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  for (int b = 0; b < 3; ++b)
+    if (!make(&P->map_c[b], P->buf[b], box_c) || !make(&P->map_o[b], P->buf[b], box_i))
+      return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
+  if (!make(&P->map_f, P->fact, box_i))
+    return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
+  P->maps_by = P->by;
+  return AWC_OK;
+}
+
+template <typename T, int BY>
+constexpr int tma_smem() {
+  return kTmaStages * awc::TmaStage<T, BY>::BYTES + kTmaStages * 8;
+}
+
+// Opts every TMA-variant instantiation into its dynamic shared memory size
+// on the current device (done at context creation, outside any capture).
+int init_kernel_attrs(std::string* err) {
+#define AWC_ATTR(T, BY)                                                                    \
+  CUDA_TRY(err, cudaFuncSetAttribute(awc::step3d_tma<T, BY, kTmaStages>,                   \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,          \
+                                     tma_smem<T, BY>()))
+  AWC_ATTR(float, 4);
+  AWC_ATTR(float, 8);
+  AWC_ATTR(float, 16);
+  AWC_ATTR(double, 4);
+  AWC_ATTR(double, 8);
+  AWC_ATTR(double, 16);
+#undef AWC_ATTR
+  return AWC_OK;
+}
+
+template <typename T, int BY>
+int launch_tma(awc_plan* P, int64_t it, const awc::StepParams<T>& S, dim3 grid, cudaStream_t st) {
+  awc::step3d_tma<T, BY, kTmaStages><<<grid, dim3(32, BY), tma_smem<T, BY>(), st>>>(
+      P->map_c[(it + 1) % 3], P->map_o[it % 3], P->map_f, S);
+  return AWC_OK;
 }
 
 template <typename T>
 int launch_step(awc_plan* P, int64_t it, cudaStream_t st) {
   const awc_problem* p = &P->p;
   awc::StepParams<T> S = step_params<T>(P, it);
-  const int ix = (int)(p->nx - 2), iy = (int)(p->ny - 2);
-  if (p->ndim == 3) {
-    const int iz = (int)(p->nz - 2);
-    dim3 grid((ix + 31) / 32, (iy + P->by - 1) / P->by, (iz + P->zchunk - 1) / P->zchunk);
+  const dim3 grid = step_grid(P);
+  int rc = AWC_OK;
+  if (p->ndim == 3 && P->kernel == 1) {
+    switch (P->by) {
+      case 4: rc = launch_tma<T, 4>(P, it, S, grid, st); break;
+      case 8: rc = launch_tma<T, 8>(P, it, S, grid, st); break;
+      case 16: rc = launch_tma<T, 16>(P, it, S, grid, st); break;
+      default: return set_err(&P->ctx->err, AWC_ERR_INVALID, "unsupported tile height %d", P->by);
+    }
+  } else if (p->ndim == 3) {
     switch (P->by) {
       case 4: awc::step3d<T, 4><<<grid, dim3(32, 4), 0, st>>>(S); break;
       case 8: awc::step3d<T, 8><<<grid, dim3(32, 8), 0, st>>>(S); break;
@@ -398,14 +613,9 @@ int launch_step(awc_plan* P, int64_t it, cudaStream_t st) {
       default: return set_err(&P->ctx->err, AWC_ERR_INVALID, "unsupported tile height %d", P->by);
     }
   } else {
-    dim3 block(32, 8);
-    dim3 grid((ix + 31) / 32, (iy + 7) / 8);
-    awc::step2d<T><<<grid, block, 0, st>>>(S);
+    awc::step2d<T><<<grid, dim3(32, 8), 0, st>>>(S);
   }
-  if (p->nsrc > 0 || p->nrec > 0) {
-    const int threads = (int)std::min<int64_t>(1024, ((std::max(p->nsrc, p->nrec) + 31) / 32) * 32);
-    awc::inject_record<T><<<1, threads, 0, st>>>(S.pnew, io_params<T>(P), (int)it);
-  }
+  if (rc) return rc;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return set_err(&P->ctx->err, AWC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
@@ -420,10 +630,18 @@ int launch_range(awc_plan* P, int64_t start, int64_t n, cudaStream_t st) {
   return AWC_OK;
 }
 
+// Everything a launch sequence depends on besides the step index.
+int prepare_launch(awc_plan* P) {
+  int rc;
+  if ((rc = ensure_io(P))) return rc;
+  if (P->p.ndim == 3 && P->kernel == 1 && (rc = ensure_maps(P))) return rc;
+  return AWC_OK;
+}
+
 uint64_t config_key(const awc_plan* P) {
-  uint64_t k = (uint64_t)P->by | ((uint64_t)P->zchunk << 8);
+  uint64_t k = launch_shape(P) ^ ((uint64_t)(P->io_version & 0xffff) << 24);
   for (int a = 0; a < 3; ++a)
-    for (int s = 0; s < 2; ++s) k |= (uint64_t)P->active[a][s] << (40 + 2 * a + s);
+    for (int s = 0; s < 2; ++s) k ^= (uint64_t)P->active[a][s] << (48 + 2 * a + s);
   return k;
 }
 
@@ -459,27 +677,63 @@ int get_graph(awc_plan* P, int64_t start, int64_t n, cudaGraphExec_t* out) {
   return AWC_OK;
 }
 
-// Default launch shape: tile 32 x 8 columns; z chunks so that one wave of
-// resident blocks covers the grid (148 SMs on B200).
-void default_tuning(awc_plan* P) {
+int occupancy(const awc_plan* P, int kernel, int by) {
+  int occ = 0;
+  const bool f64 = P->p.precision == AWC_F64;
+  auto reg = [&](auto fn) { cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * by, 0); };
+  auto tma = [&](auto fn, int smem) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * by, smem);
+  };
+#define AWC_SMEM(T, BY) tma_smem<T, BY>()
+  if (kernel == 1) {
+    if (f64) {
+      if (by == 4) tma(awc::step3d_tma<double, 4, kTmaStages>, AWC_SMEM(double, 4));
+      if (by == 8) tma(awc::step3d_tma<double, 8, kTmaStages>, AWC_SMEM(double, 8));
+      if (by == 16) tma(awc::step3d_tma<double, 16, kTmaStages>, AWC_SMEM(double, 16));
+    } else {
+      if (by == 4) tma(awc::step3d_tma<float, 4, kTmaStages>, AWC_SMEM(float, 4));
+      if (by == 8) tma(awc::step3d_tma<float, 8, kTmaStages>, AWC_SMEM(float, 8));
+      if (by == 16) tma(awc::step3d_tma<float, 16, kTmaStages>, AWC_SMEM(float, 16));
+    }
+  } else {
+    if (f64) {
+      if (by == 4) reg(awc::step3d<double, 4>);
+      if (by == 8) reg(awc::step3d<double, 8>);
+      if (by == 16) reg(awc::step3d<double, 16>);
+    } else {
+      if (by == 4) reg(awc::step3d<float, 4>);
+      if (by == 8) reg(awc::step3d<float, 8>);
+      if (by == 16) reg(awc::step3d<float, 16>);
+    }
+  }
+#undef AWC_SMEM
+  cudaGetLastError();
+  return occ > 0 ? occ : 1;
+}
+
+// z chunk that spreads the tiles of one (kernel, tile height) over about
+// `waves` rounds of resident blocks.
+int32_t chunk_for(const awc_plan* P, int kernel, int by, double waves) {
   const awc_problem* p = &P->p;
+  const int64_t iz = p->nz - 2;
+  const int64_t tiles = ((p->nx - 2) / 32 + 1) * ((p->ny - 2 + by - 1) / by);
+  const int64_t resident = (int64_t)P->ctx->num_sms * occupancy(P, kernel, by);
+  int64_t nch = (int64_t)std::llround(waves * (double)resident / (double)std::max<int64_t>(tiles, 1));
+  nch = std::max<int64_t>(1, std::min<int64_t>(nch, iz));
+  return (int32_t)((iz + nch - 1) / nch);
+}
+
+// Default launch shape: 3D uses the TMA pipeline with 32 x 8 tiles and one
+// wave of resident blocks; the autotuner refines it.
+void default_tuning(awc_plan* P) {
   P->by = 8;
-  if (p->ndim != 3) {
+  if (P->p.ndim != 3) {
+    P->kernel = 0;
     P->zchunk = 1;
     return;
   }
-  const int64_t ix = p->nx - 2, iy = p->ny - 2, iz = p->nz - 2;
-  const int64_t tiles = ((ix + 31) / 32) * ((iy + P->by - 1) / P->by);
-  int occ = 0;
-  if (p->precision == AWC_F64)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, awc::step3d<double, 8>, 256, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, awc::step3d<float, 8>, 256, 0);
-  if (occ <= 0) occ = 4;
-  const int64_t resident = (int64_t)P->ctx->num_sms * occ;
-  int64_t nch = std::max<int64_t>(1, resident / std::max<int64_t>(tiles, 1));
-  nch = std::min<int64_t>(nch, iz);
-  P->zchunk = (int32_t)((iz + nch - 1) / nch);
+  P->kernel = tensor_map_encoder() ? 1 : 0;
+  P->zchunk = chunk_for(P, P->kernel, P->by, 1.0);
 }
 
 int forward_impl(awc_ctx* C, const awc_problem* p, const double* vel, const double* coeffs,
@@ -493,11 +747,11 @@ int forward_impl(awc_ctx* C, const awc_problem* p, const double* vel, const doub
     return set_err(err, AWC_ERR_INVALID, "dt2srctf is NULL");
   if ((rc = check_positions(p, possrcs, p->nsrc, "source", err))) return rc;
   if ((rc = check_positions(p, posrecs, p->nrec, "receiver", err))) return rc;
+  CUDA_TRY(err, cudaSetDevice(C->device));
   awc_plan* P = new awc_plan();
   P->ctx = C;
   P->p = *p;
   if (p->ndim == 2) P->p.nz = 1;
-  CUDA_TRY(err, cudaSetDevice(C->device));
   if ((rc = plan_alloc(P)) || (rc = plan_upload(P, vel, coeffs, possrcs, dt2srctf, posrecs))) {
     delete P;
     return rc;
@@ -511,6 +765,19 @@ bool same_shape(const awc_problem& a, const awc_problem& b) {
   return a.ndim == b.ndim && a.precision == b.precision && a.nx == b.nx && a.ny == b.ny &&
          (a.ndim == 2 || a.nz == b.nz) && a.halo == b.halo && a.nt == b.nt && a.nsrc == b.nsrc &&
          a.nrec == b.nrec;
+}
+
+// Reads and clears the device error flag after the stream has drained.
+int check_device_flag(awc_plan* P) {
+  awc_ctx* C = P->ctx;
+  int32_t flag = 0;
+  CUDA_TRY(&C->err, cudaMemcpyAsync(&flag, P->err_flag, 4, cudaMemcpyDeviceToHost, C->stream));
+  CUDA_TRY(&C->err, cudaStreamSynchronize(C->stream));
+  if (flag) {
+    CUDA_TRY(&C->err, cudaMemsetAsync(P->err_flag, 0, 4, C->stream));
+    return set_err(&C->err, AWC_ERR_TIMEOUT, "a bounded wait on a pipeline barrier ran out");
+  }
+  return AWC_OK;
 }
 
 }  // namespace
@@ -589,6 +856,7 @@ int awc_create(awc_ctx** out, int32_t device) {
     return set_err(nullptr, AWC_ERR_NODEVICE, "device %d is sm_%d%d; this build targets sm_100a",
                    device, prop.major, prop.minor);
   CUDA_TRY(nullptr, cudaSetDevice(device));
+  if (int rc = init_kernel_attrs(nullptr)) return rc;
   awc_ctx* C = new awc_ctx();
   C->device = device;
   C->num_sms = prop.multiProcessorCount;
@@ -621,6 +889,13 @@ float awc_last_run_ms(const awc_ctx* ctx) { return ctx ? ctx->last_run_ms : 0.f;
 
 void* awc_ctx_stream(const awc_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+int awc_ctx_set_autotune(awc_ctx* ctx, int64_t steps) {
+  if (!ctx) return set_err(nullptr, AWC_ERR_INVALID, "ctx is NULL");
+  if (steps < 0) return set_err(&ctx->err, AWC_ERR_INVALID, "steps must be >= 0");
+  ctx->autotune_steps = steps;
+  return AWC_OK;
+}
+
 int awc_plan_create(awc_ctx* ctx, const awc_problem* p, const double* vel, const double* coeffs,
                     const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
                     awc_plan** out) {
@@ -643,7 +918,7 @@ int awc_plan_reset(awc_plan* P) {
   cudaStream_t st = C->stream;
   CUDA_TRY(&C->err, cudaSetDevice(C->device));
   for (int b = 0; b < 3; ++b)
-    CUDA_TRY(&C->err, cudaMemsetAsync(P->buf[b], 0, P->N * P->esz, st));
+    CUDA_TRY(&C->err, cudaMemsetAsync(P->buf[b], 0, P->NP * P->esz, st));
   for (int a = 0; a < p->ndim; ++a)
     for (int s = 0; s < 2; ++s) {
       const int64_t cs = cross_section(p, a);
@@ -667,6 +942,7 @@ int awc_plan_run(awc_plan* P, int64_t nsteps, int32_t use_graph, float* ms) {
   if (ms) *ms = 0.f;
   if (n <= 0) return AWC_OK;
   int rc;
+  if ((rc = prepare_launch(P))) return rc;
   cudaGraphExec_t ex = nullptr;
   if (use_graph && (rc = get_graph(P, P->step, n, &ex))) return rc;
   CUDA_TRY(&C->err, cudaEventRecord(C->ev0, C->stream));
@@ -679,7 +955,7 @@ int awc_plan_run(awc_plan* P, int64_t nsteps, int32_t use_graph, float* ms) {
   CUDA_TRY(&C->err, cudaEventSynchronize(C->ev1));
   if (ms) CUDA_TRY(&C->err, cudaEventElapsedTime(ms, C->ev0, C->ev1));
   P->step += n;
-  return AWC_OK;
+  return check_device_flag(P);
 }
 
 int64_t awc_plan_step(const awc_plan* P) { return P ? P->step : -1; }
@@ -707,21 +983,84 @@ int awc_plan_field(awc_plan* P, double* out) {
   CUDA_TRY(&C->err, cudaSetDevice(C->device));
   // after s steps the latest new field is buf[(s+1)%3] (the reference's pcur)
   const void* cur = P->buf[(P->step + 1) % 3];
-  if (P->p.precision == AWC_F64) {
-    CUDA_TRY(&C->err, cudaMemcpyAsync(out, cur, P->N * 8, cudaMemcpyDeviceToHost, C->stream));
-  } else {
-    const int blocks = (int)std::min<int64_t>((P->N + 255) / 256, (int64_t)C->num_sms * 16);
-    awc::widen<float><<<blocks, 256, 0, C->stream>>>((const float*)cur, P->staging, P->N);
-    CUDA_TRY(&C->err, cudaGetLastError());
-    CUDA_TRY(&C->err, cudaMemcpyAsync(out, P->staging, P->N * 8, cudaMemcpyDeviceToHost, C->stream));
-  }
+  const int blocks = grid_for(C, P->N, 256);
+  if (P->p.precision == AWC_F64)
+    awc::unpitch<double><<<blocks, 256, 0, C->stream>>>((const double*)cur, P->staging, P->N, P->p.nx, P->px);
+  else
+    awc::unpitch<float><<<blocks, 256, 0, C->stream>>>((const float*)cur, P->staging, P->N, P->p.nx, P->px);
+  CUDA_TRY(&C->err, cudaGetLastError());
+  CUDA_TRY(&C->err, cudaMemcpyAsync(out, P->staging, P->N * 8, cudaMemcpyDeviceToHost, C->stream));
   CUDA_TRY(&C->err, cudaStreamSynchronize(C->stream));
   return AWC_OK;
 }
 
-int32_t awc_plan_launches_per_step(const awc_plan* P) {
-  if (!P) return 0;
-  return 1 + ((P->p.nsrc > 0 || P->p.nrec > 0) ? 1 : 0);
+int32_t awc_plan_launches_per_step(const awc_plan* P) { return P ? 1 : 0; }
+
+int awc_plan_set_launch(awc_plan* P, int32_t kernel, int32_t tile_y, int32_t zchunk) {
+  if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
+  if (kernel != 0 && kernel != 1) return set_err(&P->ctx->err, AWC_ERR_INVALID, "kernel must be 0 or 1");
+  if (kernel == 1 && !tensor_map_encoder())
+    return set_err(&P->ctx->err, AWC_ERR_INVALID, "the TMA kernel needs cuTensorMapEncodeTiled");
+  if (tile_y != 4 && tile_y != 8 && tile_y != 16)
+    return set_err(&P->ctx->err, AWC_ERR_INVALID, "tile_y must be 4, 8 or 16");
+  if (zchunk < 1) return set_err(&P->ctx->err, AWC_ERR_INVALID, "zchunk must be >= 1");
+  if (P->p.ndim == 3) {
+    P->kernel = kernel;
+    P->by = tile_y;
+    P->zchunk = (int32_t)std::min<int64_t>(zchunk, P->p.nz - 2);
+  }
+  return AWC_OK;
+}
+
+int awc_plan_get_launch(const awc_plan* P, int32_t* kernel, int32_t* tile_y, int32_t* zchunk) {
+  if (!P || !kernel || !tile_y || !zchunk) return set_err(nullptr, AWC_ERR_INVALID, "NULL argument");
+  *kernel = P->kernel;
+  *tile_y = P->by;
+  *zchunk = P->zchunk;
+  return AWC_OK;
+}
+
+int awc_plan_autotune(awc_plan* P, int64_t steps, float* best_ms_per_step) {
+  if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
+  awc_ctx* C = P->ctx;
+  if (steps < 1) return set_err(&C->err, AWC_ERR_INVALID, "steps must be >= 1");
+  if (P->p.ndim != 3 || P->p.nt < 1) {
+    if (best_ms_per_step) *best_ms_per_step = 0.f;
+    return AWC_OK;
+  }
+  const int64_t n = std::min<int64_t>(steps, P->p.nt);
+  struct Cand { int32_t kernel, by, zchunk; };
+  std::vector<Cand> cands;
+  const int nk = tensor_map_encoder() ? 2 : 1;
+  for (int kernel = nk - 1; kernel >= 0; --kernel)
+    for (int by : {4, 8, 16})
+      for (double waves : {0.5, 1.0, 2.0, 4.0}) {
+        const Cand c{kernel, by, chunk_for(P, kernel, by, waves)};
+        bool dup = false;
+        for (const Cand& d : cands) dup = dup || (d.kernel == c.kernel && d.by == c.by && d.zchunk == c.zchunk);
+        if (!dup) cands.push_back(c);
+      }
+  float best = 1e30f;
+  Cand win = {P->kernel, P->by, P->zchunk};
+  int rc;
+  for (const Cand& c : cands) {
+    P->kernel = c.kernel;
+    P->by = c.by;
+    P->zchunk = c.zchunk;
+    if ((rc = awc_plan_reset(P)) || (rc = awc_plan_run(P, 1, 0, nullptr))) return rc;  // warm-up
+    float ms = 0.f;
+    if ((rc = awc_plan_run(P, n, 0, &ms))) return rc;
+    const float per = ms / (float)n;
+    if (per < best) {
+      best = per;
+      win = c;
+    }
+  }
+  P->kernel = win.kernel;
+  P->by = win.by;
+  P->zchunk = win.zchunk;
+  if (best_ms_per_step) *best_ms_per_step = best;
+  return awc_plan_reset(P);
 }
 
 int awc_forward(awc_ctx* ctx, const awc_problem* p, const double* vel, const double* coeffs,
@@ -757,6 +1096,12 @@ int awc_forward(awc_ctx* ctx, const awc_problem* p, const double* vel, const dou
     }
   } else {
     if ((rc = forward_impl(ctx, p, vel, coeffs, possrcs, dt2srctf, posrecs, &P))) return rc;
+    // a new 3D shape: pick its launch shape once, on its own data
+    if (p->ndim == 3 && ctx->autotune_steps > 0 && p->nt >= 100 &&
+        (rc = awc_plan_autotune(P, ctx->autotune_steps, nullptr))) {
+      delete P;
+      return rc;
+    }
   }
   ctx->cache.push_back(P);
   while (ctx->cache.size() > 2) {

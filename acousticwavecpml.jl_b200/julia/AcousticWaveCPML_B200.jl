@@ -1,0 +1,144 @@
+"""
+    AcousticWaveCPML_B200
+
+Drop-in replacement of the GPU time loop of AcousticWaveCPML.jl's
+`Acoustic2D_CUDA.solve2D` and `Acoustic3D_CUDA.solve3D`
+(src/shared/acoustic_2D_xPU.jl:133-445, src/shared/acoustic_3D_xPU.jl:169-545).
+The host setup below is the reference's (dt, nt, CPML coefficients, source time
+functions, nearest-node snapping, assertions); the time loop runs in
+libawcpml.so through `awc_forward` (include/awcpml.h).
+
+Load it next to the reference package:
+
+    using AcousticWaveCPML
+    include("AcousticWaveCPML_B200.jl")
+    pend = AcousticWaveCPML_B200.solve3D(lx, ly, lz, lt, vel, srcs, recs; halo=20)
+
+Set `ENV["AWCPML_LIB"]` to the path of libawcpml.so if it is not in the
+default location (../lib/libawcpml.so relative to this file).
+"""
+module AcousticWaveCPML_B200
+
+import ..AcousticWaveCPML: Sources, Receivers, calc_Kab_CPML
+
+export solve2D, solve3D
+
+const LIBAWCPML = get(ENV, "AWCPML_LIB", joinpath(@__DIR__, "..", "lib", "libawcpml.so"))
+
+const AWC_F32 = Int32(1)
+const AWC_F64 = Int32(2)
+
+# awc_problem (include/awcpml.h)
+struct AwcProblem
+    ndim::Int32
+    precision::Int32
+    nx::Int64
+    ny::Int64
+    nz::Int64
+    halo::Int32
+    freetop::Int32
+    dx::Float64
+    dy::Float64
+    dz::Float64
+    dt::Float64
+    nt::Int64
+    nsrc::Int64
+    nrec::Int64
+end
+
+const _CTX = Ref{Ptr{Cvoid}}(C_NULL)
+
+function context(device::Integer=0)
+    if _CTX[] == C_NULL
+        out = Ref{Ptr{Cvoid}}(C_NULL)
+        rc = ccall((:awc_create, LIBAWCPML), Cint, (Ref{Ptr{Cvoid}}, Int32), out, Int32(device))
+        check(rc, C_NULL)
+        _CTX[] = out[]
+        atexit(() -> ccall((:awc_destroy, LIBAWCPML), Cvoid, (Ptr{Cvoid},), _CTX[]))
+    end
+    return _CTX[]
+end
+
+function check(rc::Integer, ctx::Ptr{Cvoid})
+    if rc != 0
+        msg = unsafe_string(ccall((:awc_last_error, LIBAWCPML), Cstring, (Ptr{Cvoid},), ctx))
+        rc == -1 ? throw(ArgumentError(msg)) : error("libawcpml error $rc: $msg")
+    end
+    return nothing
+end
+
+# CPML block of solve2D/solve3D (acoustic_3D_xPU.jl:207-230), packed per axis
+# as awc_coeffs_len documents: a_l a_r bK_l bK_r a_hl a_hr bK_hl bK_hr.
+function packed_coeffs(halo, dt, ds, vel_max, rcoef, f0, freetop)
+    alpha_max, npower, K_max = π * f0, 2.0, 1.0
+    out = Float64[]
+    for (ax, d) in enumerate(ds)
+        d0 = -(npower + 1) * vel_max * log(rcoef) / (2.0 * (halo * d))
+        a_l, a_r, b_K_l, b_K_r = calc_Kab_CPML(halo, dt, npower, d0, alpha_max, K_max, "ongrd")
+        a_hl, a_hr, b_K_hl, b_K_hr = calc_Kab_CPML(halo, dt, npower, d0, alpha_max, K_max, "halfgrd")
+        if ax == 2 && freetop
+            a_l .= 0.0; a_hl .= 0.0; b_K_l .= 1.0; b_K_hl .= 1.0
+        end
+        append!(out, a_l, a_r, b_K_l, b_K_r, a_hl, a_hr, b_K_hl, b_K_hr)
+    end
+    return out
+end
+
+function _solve(ls::NTuple{N,Real}, lt::Real, vel::Array{<:Real,N}, srcs::Sources,
+                recs::Receivers; halo::Integer=20, rcoef::Real=0.0001, ppw::Real=10.0,
+                freetop::Bool=true, precision::Symbol=:f64, dt=nothing, nt=nothing,
+                device::Integer=0) where {N}
+    f0 = srcs.freqdomain
+    vel_max = maximum(vel)
+    ns = size(vel)
+    ds = ntuple(a -> ls[a] / (ns[a] - 1), N)
+    dt = dt === nothing ? sqrt(N) / (vel_max * sum(1 ./ ds)) / 2 : Float64(dt)
+    nt = nt === nothing ? ceil(Int, lt / dt) : Int(nt)
+    times = collect(range(0.0, step=dt, length=nt))
+    @assert sqrt(sum(ds .^ 2)) <= vel_max / (ppw * f0) "Not enough points per wavelength!"
+    dt2srctf = zeros(nt, srcs.n)
+    for s = 1:srcs.n
+        dt2srctf[:, s] .= (dt^2 / prod(ds)) .* srcs.srctfs[s].(times, srcs.t0s[s], f0)
+    end
+    snap(pos) = round.(Int64, pos ./ reshape(collect(ds), 1, N) .+ 1, RoundNearestTiesUp)
+    possrcs, posrecs = snap(srcs.positions), snap(recs.positions)
+    @assert all(all(1 .<= possrcs[:, a] .<= ns[a]) for a in 1:N) "At least one source is not inside the model!"
+    @assert all(all(1 .<= posrecs[:, a] .<= ns[a]) for a in 1:N) "At least one receiver is not inside the model!"
+    coeffs = packed_coeffs(halo, dt, ds, vel_max, rcoef, f0, freetop)
+    prob = AwcProblem(Int32(N), precision == :f32 ? AWC_F32 : AWC_F64, ns[1], ns[2],
+                      N == 3 ? ns[3] : 1, Int32(halo), Int32(freetop), ds[1], ds[2],
+                      N == 3 ? ds[3] : 1.0, dt, nt, srcs.n, recs.n)
+    traces = zeros(Float64, nt, recs.n)
+    pend = zeros(Float64, ns)
+    ctx = context(device)
+    rc = ccall((:awc_forward, LIBAWCPML), Cint,
+               (Ptr{Cvoid}, Ref{AwcProblem}, Ptr{Float64}, Ptr{Float64}, Ptr{Int64},
+                Ptr{Float64}, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}),
+               ctx, prob, Array{Float64}(vel), coeffs, possrcs, dt2srctf, posrecs, traces, pend)
+    check(rc, ctx)
+    recs.seismograms = traces
+    return pend
+end
+
+"""
+    solve2D(lx, ly, lt, vel, srcs, recs; halo=20, rcoef=0.0001, ppw=10.0, freetop=true,
+            precision=:f64, dt=nothing, nt=nothing, device=0)
+
+`Acoustic2D_CUDA.solve2D` with the time loop on a B200. Returns the final
+pressure field and fills `recs.seismograms`. `precision=:f32` selects the
+production single-precision build; `dt`/`nt` fix the time step explicitly.
+"""
+solve2D(lx::Real, ly::Real, lt::Real, vel::Matrix{<:Real}, srcs::Sources, recs::Receivers; kw...) =
+    _solve((lx, ly), lt, vel, srcs, recs; kw...)
+
+"""
+    solve3D(lx, ly, lz, lt, vel, srcs, recs; halo=20, rcoef=0.0001, ppw=10.0, freetop=true,
+            precision=:f64, dt=nothing, nt=nothing, device=0)
+
+`Acoustic3D_CUDA.solve3D` with the time loop on a B200 (depth on the second
+axis, free top at j = 1).
+"""
+solve3D(lx::Real, ly::Real, lz::Real, lt::Real, vel::Array{<:Real,3}, srcs::Sources,
+        recs::Receivers; kw...) = _solve((lx, ly, lz), lt, vel, srcs, recs; kw...)
+
+end # module

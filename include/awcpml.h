@@ -96,6 +96,10 @@ float awc_last_run_ms(const awc_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t), on which every copy and kernel
  * of the context is ordered; callers may record their own events on it. */
 void* awc_ctx_stream(const awc_ctx* ctx);
+/* Steps per candidate with which awc_forward autotunes the launch shape of
+ * each new 3D problem shape (nt >= 100) before its first solve; 0 disables
+ * it. Default 10. The choice is cached with the plan. */
+int awc_ctx_set_autotune(awc_ctx* ctx, int64_t steps);
 
 /* The forward solve (the time loop of acoustic_3D_xPU.jl:392-409 and the
  * returns at :541-544; 2D acoustic_2D_xPU.jl:327-343, :441-444).
@@ -140,6 +144,18 @@ int awc_plan_traces(awc_plan* plan, double* traces);
 int awc_plan_field(awc_plan* plan, double* p);
 /* Number of kernel launches one time step issues (for launch accounting). */
 int32_t awc_plan_launches_per_step(const awc_plan* plan);
+/* Launch shape of the 3D step kernel. kernel 0 keeps the z neighbours in a
+ * register queue; kernel 1 streams z planes through a TMA + mbarrier pipeline
+ * in shared memory. `tile_y` rows (4, 8 or 16) of 32-wide x tiles per block
+ * and `zchunk` z planes streamed per block (>= 1). Every shape gives the
+ * same results; only the speed differs. The state is kept. 2D plans ignore
+ * the call. */
+int awc_plan_set_launch(awc_plan* plan, int32_t kernel, int32_t tile_y, int32_t zchunk);
+int awc_plan_get_launch(const awc_plan* plan, int32_t* kernel, int32_t* tile_y, int32_t* zchunk);
+/* Times `steps` time steps of every candidate launch shape on this plan's own
+ * data, keeps the fastest, and resets the state. Writes the best time per
+ * step [ms] to best_ms_per_step when not NULL. */
+int awc_plan_autotune(awc_plan* plan, int64_t steps, float* best_ms_per_step);
 
 #ifdef __cplusplus
 }

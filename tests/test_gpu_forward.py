@@ -86,7 +86,9 @@ def small3d(n=(40, 34, 28), halo=6, freetop=True, srcs=None, recs=None, lt=0.2, 
     if recs is None:
         recs = [[(i - 1) * d, 3 * d, (k - 1) * d] for i in (3, nx // 2, nx - 3) for k in (4, nz - 4)]
         recs += [[(nx // 3) * d, (ny - 5) * d, (nz // 3) * d]]
-    return (L, lt, vel, srcs, [4 / f0] * len(srcs), f0, recs,
+    # the wavelet peaks at t0 = 0.05 s, inside every case's lt, so the fields
+    # are far above FP32's range floor from the first steps on
+    return (L, lt, vel, srcs, [0.05] * len(srcs), f0, recs,
             dict(halo=halo, rcoef=1e-4, freetop=freetop, check_ppw=False))
 
 
@@ -174,6 +176,55 @@ def test_plan_graph_eager_and_split_runs_agree(pkg, ctx):
     np.testing.assert_array_equal(p_g, p_e)
     np.testing.assert_array_equal(tr_g, tr_s)
     np.testing.assert_array_equal(p_g, p_s)
+
+
+def test_launch_shapes_give_identical_results(pkg, ctx):
+    """Every tile shape / z chunking computes the same numbers; sources and
+    receivers (interior, rim, shared nodes) land in the right blocks."""
+    srcs_pos = [[200.0, 80.0, 140.0], [200.0, 80.0, 140.0], [0.0, 50.0, 60.0],
+                [390.0, 200.0, 10.0]]
+    recs_pos = [[200.0, 80.0, 140.0], [0.0, 50.0, 60.0], [100.0, 330.0, 270.0],
+                [310.0, 10.0, 20.0], [10.0, 20.0, 260.0]]
+    lengths, lt, vel, sp, t0s, f0, rp, kw = small3d(srcs=srcs_pos, recs=recs_pos, freetop=False)
+    kw = dict(kw)
+    kw.pop("check_ppw")
+    srcs = pkg.Sources(sp, t0s, [pkg.rickersource1D] * len(t0s), f0)
+    recs = pkg.Receivers(rp)
+    for prec in ("f32", "f64"):
+        s = pkg.prepare(lengths, lt, vel, srcs, recs, precision=prec, ppw=1e-9, **kw)
+        plan = ctx.plan(s["problem"], s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"],
+                        s["posrecs"])
+        plan.run()
+        ref_t, ref_p = plan.traces(), plan.field()
+        assert np.abs(ref_t).max() > 0
+        shapes = [(k, ty, zc) for k in (0, 1)
+                  for ty, zc in ((4, 1), (4, 7), (8, 3), (16, 5), (16, 100), (8, 26))]
+        for kn, ty, zc in shapes:
+            plan.set_launch(kn, ty, zc)
+            plan.reset()
+            plan.run()
+            np.testing.assert_array_equal(plan.traces(), ref_t)
+            np.testing.assert_array_equal(plan.field(), ref_p)
+        plan.close()
+
+
+def test_autotune_keeps_results(pkg, ctx):
+    lengths, lt, vel, sp, t0s, f0, rp, kw = small3d(freetop=True)
+    kw = dict(kw)
+    kw.pop("check_ppw")
+    srcs = pkg.Sources(sp, t0s, [pkg.rickersource1D] * len(t0s), f0)
+    recs = pkg.Receivers(rp)
+    s = pkg.prepare(lengths, lt, vel, srcs, recs, precision="f32", ppw=1e-9, **kw)
+    plan = ctx.plan(s["problem"], s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"], s["posrecs"])
+    plan.run()
+    ref = plan.traces()
+    best = plan.autotune(5)
+    assert best > 0 and plan.step == 0
+    kn, ty, zc = plan.get_launch()
+    assert kn in (0, 1) and ty in (4, 8, 16) and zc >= 1
+    plan.run()
+    np.testing.assert_array_equal(plan.traces(), ref)
+    plan.close()
 
 
 def test_forward_reuses_cached_plan(pkg, oracle, ctx):
