@@ -133,16 +133,16 @@ class Plan:
     def launches_per_step(self):
         return int(_lib.lib().awc_plan_launches_per_step(self._h))
 
-    def set_launch(self, kernel, tile_y, zchunk):
-        """3D launch shape: kernel 0 (register queue) or 1 (TMA pipeline)."""
-        check(_lib.lib().awc_plan_set_launch(self._h, int(kernel), int(tile_y), int(zchunk)),
-              self.ctx.handle)
+    def set_launch(self, tile_y, zchunk, band_zchunk=10):
+        """3D launch shape: core tile rows, core z chunk, band-kernel z chunk."""
+        check(_lib.lib().awc_plan_set_launch(self._h, int(tile_y), int(zchunk),
+                                             int(band_zchunk)), self.ctx.handle)
 
     def get_launch(self):
-        kn, ty, zc = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-        check(_lib.lib().awc_plan_get_launch(self._h, ctypes.byref(kn), ctypes.byref(ty),
-                                             ctypes.byref(zc)), self.ctx.handle)
-        return kn.value, ty.value, zc.value
+        ty, zc, bz = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(_lib.lib().awc_plan_get_launch(self._h, ctypes.byref(ty), ctypes.byref(zc),
+                                             ctypes.byref(bz)), self.ctx.handle)
+        return ty.value, zc.value, bz.value
 
     def autotune(self, steps=20):
         """Picks the fastest launch shape on this plan's data; resets the state.

@@ -155,7 +155,10 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-constexpr int kTmaStages = 6;  // pipeline depth of step3d_tma (3 planes ahead)
+// Pipeline depth of the 3D step kernel: S stages let the TMA loads run S-3
+// planes ahead of the plane being computed.
+template <typename T>
+constexpr int stages() { return sizeof(T) == 4 ? 6 : 4; }
 
 }  // namespace
 
@@ -163,7 +166,9 @@ struct awc_ctx {
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;  // second branch of a 3D step (the shell kernel)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   float last_run_ms = 0.f;
   int64_t autotune_steps = 10;   // per candidate, for new 3D plans of awc_forward
@@ -191,20 +196,32 @@ struct awc_plan {
   int32_t* rec_off = nullptr;
   int32_t* rec_ids = nullptr;
   std::vector<awc::IoRim> io_nodes;  // host copy: node, source group, receiver group
-  int32_t* io_blk_off = nullptr;
-  int64_t io_blk_cap = 0;
-  int4* io_ent = nullptr;
+  struct IoSet {                     // one kernel's per-block source/receiver lists
+    int32_t* blk_off = nullptr;
+    int64_t cap = 0;
+    int4* ent = nullptr;
+    int32_t do_rim = 0;
+  } io_k[2];                         // [0] 3D core or 2D kernel, [1] 3D shell kernel
   awc::IoRim* io_rim = nullptr;
   int32_t io_nrim = 0;
   uint64_t io_shape = ~0ull;  // launch shape io_* were built for
   uint32_t io_version = 0;
+  // 3D regions: the band-free core box and the shell boxes around it
+  bool has_core = false;
+  awc::Box core{};
+  int32_t core_x = 0;
+  int32_t nbox = 0;
+  awc::Box box[6] = {};
+  int32_t box_blk[7] = {};
+  int32_t szc = 10;  // z planes per block of the band kernel
   void* stf = nullptr;     // [nt][nsrc]
   void* traces = nullptr;  // [nt][nrec]
   double* staging = nullptr;
   int64_t staging_len = 0;
   std::vector<void*> allocs;
-  // launch shape: kernel 0 = register queue, 1 = TMA pipeline (3D)
-  int32_t kernel = 0, by = 8, zchunk = 1;
+  // launch shape of the 3D core kernel: tile rows (4, 8, 16; the tile is
+  // 64 x by nodes, 32 x by/2 threads) and z planes per block
+  int32_t by = 8, zchunk = 1;
   CUtensorMap map_c[3], map_o[3], map_f;
   int32_t maps_by = 0;  // tile height the tensor maps were encoded for
   // run state
@@ -243,9 +260,12 @@ struct awc_plan {
 
 namespace {
 
+// Elements of one band layer of axis `axis`: ψ/ξ of axis x are
+// (halo[+1], ny, nz); those of axes y and z are pitched like the fields,
+// (px, halo[+1], nz) and (px, ny, halo[+1]).
 int64_t cross_section(const awc_problem* p, int axis) {
-  const int64_t nz = p->ndim == 3 ? p->nz : 1;
-  return axis == 0 ? p->ny * nz : axis == 1 ? p->nx * nz : p->nx * p->ny;
+  const int64_t nz = p->ndim == 3 ? p->nz : 1, px = pitch_of(p->nx);
+  return axis == 0 ? p->ny * nz : axis == 1 ? px * nz : px * p->ny;
 }
 
 // Allocates every device buffer of a plan (shape only, contents undefined).
@@ -275,7 +295,8 @@ int plan_alloc(awc_plan* P) {
   if ((rc = P->alloc((void**)&P->src_ids, ns * 4))) return rc;
   if ((rc = P->alloc((void**)&P->rec_off, (nr + 1) * 4))) return rc;
   if ((rc = P->alloc((void**)&P->rec_ids, nr * 4))) return rc;
-  if ((rc = P->alloc((void**)&P->io_ent, (ns + nr) * sizeof(int4)))) return rc;
+  for (int kk = 0; kk < 2; ++kk)
+    if ((rc = P->alloc((void**)&P->io_k[kk].ent, (ns + nr) * sizeof(int4)))) return rc;
   if ((rc = P->alloc((void**)&P->io_rim, (ns + nr) * sizeof(awc::IoRim)))) return rc;
   if ((rc = P->alloc(&P->stf, std::max<int64_t>(p->nt * p->nsrc, 1) * P->esz))) return rc;
   if ((rc = P->alloc(&P->traces, std::max<int64_t>(p->nt * p->nrec, 1) * P->esz))) return rc;
@@ -296,6 +317,9 @@ int grid_for(const awc_ctx* C, int64_t n, int threads) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads,
                                                      (int64_t)C->num_sms * 16));
 }
+
+void make_regions(awc_plan* P);
+void box_blocks(awc_plan* P);
 
 // Uploads the inputs of one shot into an allocated plan. The copies are
 // stream-ordered on the context stream.
@@ -340,6 +364,7 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
       P->active[a][s] = (h > 0 && !trivial) ? 1 : 0;
     }
   }
+  if (p->ndim == 3) make_regions(P);
   // every node carrying sources and/or receivers, in first-appearance order
   // (sources first); its sources are summed in source order
   {
@@ -402,6 +427,8 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
   return AWC_OK;
 }
 
+// Parameters of step `it` shared by every kernel of the step; the per-kernel
+// source/receiver lists are filled by kernel_params.
 template <typename T>
 awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
   const awc_problem* p = &P->p;
@@ -445,8 +472,6 @@ awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
   S.zchunk = P->zchunk;
   S.it = (int32_t)it;
   S.err = P->err_flag;
-  S.io.blk_off = P->io_blk_off;
-  S.io.ent = P->io_ent;
   S.io.rim = P->io_rim;
   S.io.nrim = P->io_nrim;
   S.io.src_off = P->src_off;
@@ -457,74 +482,177 @@ awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
   S.io.nsrc = (int32_t)p->nsrc;
   S.io.nrec = (int32_t)p->nrec;
   S.io.traces = (T*)P->traces;
+  S.core = P->core;
+  S.core_x = P->core_x;
+  S.nbox = P->nbox;
+  for (int b2 = 0; b2 < 6; ++b2) S.box[b2] = P->box[b2];
+  for (int b2 = 0; b2 < 7; ++b2) S.box_blk[b2] = P->box_blk[b2];
+  S.shell_zchunk = P->szc;
   return S;
 }
 
-// Tile height of the current launch shape (the 2D kernel uses 8 rows).
-int tile_rows(const awc_plan* P) { return P->p.ndim == 3 ? P->by : 8; }
+template <typename T>
+void kernel_params(const awc_plan* P, int which, awc::StepParams<T>& S) {
+  S.io.blk_off = P->io_k[which].blk_off;
+  S.io.ent = P->io_k[which].ent;
+  S.do_rim = P->io_k[which].do_rim;
+}
 
-// Launch grid of the step kernel: x tiles [32 bx, 32 bx + 32) cover nodes
-// 1..nx-2, y tiles start at node 1, z chunks at plane 1.
+// Splits the interior of a 3D grid into the core box (nodes outside every
+// active CPML band: x in [halo+1, nx-halo-2] when both x sides are active,
+// and so on) and up to six disjoint shell boxes covering the rest: the two
+// z slabs over the whole x-y interior, the two y slabs over the core z range,
+// the two x slabs over the core y and z ranges.
+void make_regions(awc_plan* P) {
+  const awc_problem* p = &P->p;
+  const int64_t n[3] = {p->nx, p->ny, p->nz};
+  int64_t lo[3], hi[3];
+  bool empty = false;
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = 1;
+    hi[a] = n[a] - 2;
+    if (P->active[a][0]) lo[a] = std::max<int64_t>(lo[a], p->halo + 1);
+    if (P->active[a][1]) hi[a] = std::min<int64_t>(hi[a], n[a] - p->halo - 2);
+    empty = empty || lo[a] > hi[a];
+  }
+  P->nbox = 0;
+  auto add = [&](int64_t x0, int64_t x1, int64_t y0, int64_t y1, int64_t z0, int64_t z1) {
+    if (x0 > x1 || y0 > y1 || z0 > z1) return;
+    P->box[P->nbox++] = awc::Box{(int32_t)x0, (int32_t)x1, (int32_t)y0, (int32_t)y1,
+                                 (int32_t)z0, (int32_t)z1};
+  };
+  if (empty) {
+    P->has_core = false;
+    add(1, n[0] - 2, 1, n[1] - 2, 1, n[2] - 2);
+  } else {
+    P->has_core = true;
+    P->core = awc::Box{(int32_t)lo[0], (int32_t)hi[0], (int32_t)lo[1], (int32_t)hi[1],
+                       (int32_t)lo[2], (int32_t)hi[2]};
+    const int64_t align = 16 / (int64_t)P->esz;  // TMA x origin alignment
+    P->core_x = (int32_t)(lo[0] / align * align);
+    add(1, n[0] - 2, 1, n[1] - 2, 1, lo[2] - 1);
+    add(1, n[0] - 2, 1, n[1] - 2, hi[2] + 1, n[2] - 2);
+    add(1, n[0] - 2, 1, lo[1] - 1, lo[2], hi[2]);
+    add(1, n[0] - 2, hi[1] + 1, n[1] - 2, lo[2], hi[2]);
+    add(1, lo[0] - 1, lo[1], hi[1], lo[2], hi[2]);
+    add(hi[0] + 1, n[0] - 2, lo[1], hi[1], lo[2], hi[2]);
+  }
+  box_blocks(P);
+}
+
+// Block ranges of the band kernel: box b has 32 x 8 column tiles times
+// chunks of szc planes.
+void box_blocks(awc_plan* P) {
+  P->box_blk[0] = 0;
+  for (int b = 0; b < P->nbox; ++b) {
+    const awc::Box& B = P->box[b];
+    const int64_t blocks = (int64_t)((B.x1 - B.x0 + 32) / 32) * ((B.y1 - B.y0 + 8) / 8) *
+                           ((B.z1 - B.z0 + P->szc) / P->szc);
+    P->box_blk[b + 1] = (int32_t)(P->box_blk[b] + blocks);
+  }
+  for (int b = P->nbox; b < 6; ++b) P->box_blk[b + 1] = P->box_blk[b];
+}
+
+// Launch grid of the 2D kernel (x tiles of 32 from x = 0, y tiles of 8 rows
+// from y = 1) or of the 3D core kernel (x tiles of 64 from core_x, y tiles of
+// `by` rows from core.y0, z chunks of `zchunk` planes from core.z0).
 dim3 step_grid(const awc_plan* P) {
   const awc_problem* p = &P->p;
-  const unsigned gx = (unsigned)((p->nx - 2) / 32 + 1);
-  const unsigned gy = (unsigned)((p->ny - 2 + tile_rows(P) - 1) / tile_rows(P));
-  if (p->ndim == 3) return dim3(gx, gy, (unsigned)((p->nz - 2 + P->zchunk - 1) / P->zchunk));
-  return dim3(gx, gy, 1);
+  if (p->ndim == 2)
+    return dim3((unsigned)((p->nx - 2) / 32 + 1), (unsigned)((p->ny - 2 + 7) / 8), 1);
+  if (!P->has_core) return dim3(0, 0, 0);
+  const awc::Box& C = P->core;
+  return dim3((unsigned)((C.x1 - P->core_x) / 64 + 1), (unsigned)((C.y1 - C.y0 + P->by) / P->by),
+              (unsigned)((C.z1 - C.z0 + P->zchunk) / P->zchunk));
 }
 
 uint64_t launch_shape(const awc_plan* P) {
-  return (uint64_t)P->by | ((uint64_t)P->zchunk << 8) | ((uint64_t)P->kernel << 40);
+  return (uint64_t)P->by | ((uint64_t)P->zchunk << 8) | ((uint64_t)(P->szc & 0xff) << 40);
 }
 
-// Buckets the source/receiver nodes by the block that owns them for the
-// current launch shape: rim nodes to the rim list, interior nodes to
-// (block, plane, local thread) order.
+// Buckets the source/receiver nodes by the kernel and block that own them for
+// the current launch shape: rim nodes to the rim list; 3D nodes inside the
+// core box to the core kernel, in (block, plane, local) order; other interior
+// nodes to the shell kernel's block of their box tile; 2D nodes to the 2D
+// kernel.
 int ensure_io(awc_plan* P) {
   if (P->io_shape == launch_shape(P)) return AWC_OK;
   awc_ctx* C = P->ctx;
   const awc_problem* p = &P->p;
+  const bool d3 = p->ndim == 3;
   const dim3 g = step_grid(P);
-  const int64_t nblk = (int64_t)g.x * g.y * g.z;
-  const int tyh = tile_rows(P);
+  const int64_t nblk[2] = {(int64_t)g.x * g.y * g.z, d3 ? (int64_t)P->box_blk[P->nbox] : 0};
   std::vector<awc::IoRim> rim;
-  std::vector<std::pair<std::pair<int64_t, int64_t>, int4>> ent;  // ((blk, k*2^32+local), entry)
+  std::vector<std::pair<std::pair<int64_t, int64_t>, int4>> ent[2];  // ((blk, k*2^32+local), entry)
   for (const awc::IoRim& e : P->io_nodes) {
     const int64_t i = e.node % P->px, j = (e.node / P->px) % p->ny, k = e.node / (P->px * p->ny);
     const bool interior = i >= 1 && i <= p->nx - 2 && j >= 1 && j <= p->ny - 2 &&
-                          (p->ndim == 2 || (k >= 1 && k <= p->nz - 2));
+                          (!d3 || (k >= 1 && k <= p->nz - 2));
     if (!interior) {
       rim.push_back(e);
       continue;
     }
-    const int64_t bx = i / 32, tx = i % 32, by = (j - 1) / tyh, ty = (j - 1) % tyh;
-    const int64_t bz = p->ndim == 3 ? (k - 1) / P->zchunk : 0;
-    const int64_t blk = bx + g.x * (by + (int64_t)g.y * bz);
-    const int local = (int)(tx + 32 * ty);
-    ent.push_back({{blk, (k << 32) | local}, make_int4(local, (int)k, e.sgrp, e.rgrp)});
-  }
-  std::sort(ent.begin(), ent.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-  std::vector<int32_t> off(nblk + 1, 0);
-  std::vector<int4> flat(ent.size());
-  for (size_t n = 0; n < ent.size(); ++n) {
-    off[ent[n].first.first + 1]++;
-    flat[n] = ent[n].second;
-  }
-  for (int64_t b = 0; b < nblk; ++b) off[b + 1] += off[b];
-  if (P->io_blk_cap < nblk + 1) {
-    P->release(P->io_blk_off);
-    P->io_blk_off = nullptr;
-    P->io_blk_cap = 0;
-    int rc = P->alloc((void**)&P->io_blk_off, (nblk + 1) * 4);
-    if (rc) return rc;
-    P->io_blk_cap = nblk + 1;
+    if (!d3) {
+      const int64_t blk = i / 32 + g.x * ((j - 1) / 8);
+      const int local = (int)(i % 32 + 32 * ((j - 1) % 8));
+      ent[0].push_back({{blk, local}, make_int4(local, 0, e.sgrp, e.rgrp)});
+      continue;
+    }
+    const awc::Box& Cb = P->core;
+    if (P->has_core && i >= Cb.x0 && i <= Cb.x1 && j >= Cb.y0 && j <= Cb.y1 && k >= Cb.z0 &&
+        k <= Cb.z1) {
+      const int64_t lx = (i - P->core_x) % 64, ly = (j - Cb.y0) % P->by;
+      const int64_t blk = (i - P->core_x) / 64 +
+                          g.x * ((j - Cb.y0) / P->by + (int64_t)g.y * ((k - Cb.z0) / P->zchunk));
+      const int local = (int)(lx + 64 * ly);
+      ent[0].push_back({{blk, (k << 32) | local}, make_int4(local, (int)k, e.sgrp, e.rgrp)});
+      continue;
+    }
+    for (int b = 0; b < P->nbox; ++b) {
+      const awc::Box& B = P->box[b];
+      if (i < B.x0 || i > B.x1 || j < B.y0 || j > B.y1 || k < B.z0 || k > B.z1) continue;
+      const int64_t gx = (B.x1 - B.x0 + 32) / 32, gy = (B.y1 - B.y0 + 8) / 8;
+      const int64_t blk = P->box_blk[b] + (i - B.x0) / 32 +
+                          gx * ((j - B.y0) / 8 + gy * ((k - B.z0) / P->szc));
+      const int local = (int)((i - B.x0) % 32 + 32 * ((j - B.y0) % 8));
+      ent[1].push_back({{blk, (k << 32) | local}, make_int4(local, (int)k, e.sgrp, e.rgrp)});
+      break;
+    }
   }
   cudaStream_t st = C->stream;
-  CUDA_TRY(&C->err, cudaMemcpyAsync(P->io_blk_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st));
-  if (!flat.empty())
-    CUDA_TRY(&C->err, cudaMemcpyAsync(P->io_ent, flat.data(), flat.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  std::vector<int32_t> off[2];
+  std::vector<int4> flat[2];
+  for (int kk = 0; kk < 2; ++kk) {
+    auto& E = ent[kk];
+    std::sort(E.begin(), E.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    off[kk].assign(nblk[kk] + 1, 0);
+    flat[kk].resize(E.size());
+    for (size_t n = 0; n < E.size(); ++n) {
+      off[kk][E[n].first.first + 1]++;
+      flat[kk][n] = E[n].second;
+    }
+    for (int64_t b = 0; b < nblk[kk]; ++b) off[kk][b + 1] += off[kk][b];
+    auto& S = P->io_k[kk];
+    if (S.cap < nblk[kk] + 1) {
+      P->release(S.blk_off);
+      S.blk_off = nullptr;
+      S.cap = 0;
+      int rc = P->alloc((void**)&S.blk_off, (nblk[kk] + 1) * 4);
+      if (rc) return rc;
+      S.cap = nblk[kk] + 1;
+    }
+    CUDA_TRY(&C->err, cudaMemcpyAsync(S.blk_off, off[kk].data(), off[kk].size() * 4,
+                                      cudaMemcpyHostToDevice, st));
+    if (!flat[kk].empty())
+      CUDA_TRY(&C->err, cudaMemcpyAsync(S.ent, flat[kk].data(), flat[kk].size() * sizeof(int4),
+                                        cudaMemcpyHostToDevice, st));
+  }
+  // the rim is served by the shell kernel when there is one, else by the other
+  P->io_k[1].do_rim = d3 && P->nbox > 0 ? 1 : 0;
+  P->io_k[0].do_rim = P->io_k[1].do_rim ? 0 : 1;
   if (!rim.empty())
-    CUDA_TRY(&C->err, cudaMemcpyAsync(P->io_rim, rim.data(), rim.size() * sizeof(awc::IoRim), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(&C->err, cudaMemcpyAsync(P->io_rim, rim.data(), rim.size() * sizeof(awc::IoRim),
+                                      cudaMemcpyHostToDevice, st));
   CUDA_TRY(&C->err, cudaStreamSynchronize(st));
   P->io_nrim = (int32_t)rim.size();
   P->io_shape = launch_shape(P);
@@ -532,9 +660,9 @@ int ensure_io(awc_plan* P) {
   return AWC_OK;
 }
 
-// Tensor maps of the TMA variant: for each rotating field buffer a map with
-// the pcur box ((32 + 2A) x (BY + 2) x 1) and one with the pold box
-// (32 x BY x 1), and one for fact. Dims (nx, ny, nz), pitched strides.
+// Tensor maps of the 3D core kernel: for each rotating field buffer a map
+// with the pcur box ((64 + 2A) x (by + 2) x 1) and one with the pold box
+// (64 x by x 1), and one for fact. Dims (nx, ny, nz), pitched strides.
 int ensure_maps(awc_plan* P) {
   if (P->maps_by == P->by) return AWC_OK;
   awc_ctx* C = P->ctx;
@@ -546,8 +674,8 @@ int ensure_maps(awc_plan* P) {
   const cuuint32_t A = 16 / (cuuint32_t)P->esz;
   const cuuint64_t dims[3] = {(cuuint64_t)p->nx, (cuuint64_t)p->ny, (cuuint64_t)p->nz};
   const cuuint64_t strides[2] = {(cuuint64_t)(P->px * P->esz), (cuuint64_t)(P->px * p->ny * P->esz)};
-  const cuuint32_t box_c[3] = {32 + 2 * A, (cuuint32_t)P->by + 2, 1};
-  const cuuint32_t box_i[3] = {32, (cuuint32_t)P->by, 1};
+  const cuuint32_t box_c[3] = {64 + 2 * A, (cuuint32_t)P->by + 2, 1};
+  const cuuint32_t box_i[3] = {64, (cuuint32_t)P->by, 1};
   const cuuint32_t es[3] = {1, 1, 1};
   auto make = [&](CUtensorMap* m, void* base, const cuuint32_t* box) -> bool {
     return enc(m, dt, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -563,62 +691,75 @@ int ensure_maps(awc_plan* P) {
   return AWC_OK;
 }
 
-template <typename T, int BY>
-constexpr int tma_smem() {
-  return kTmaStages * awc::TmaStage<T, BY>::BYTES + kTmaStages * 8;
+template <typename T, int TY>
+constexpr int core_smem() {
+  return stages<T>() * awc::Tile3<T, TY>::BYTES + 2 * stages<T>() * 8 + 16;
 }
 
-// Opts every TMA-variant instantiation into its dynamic shared memory size
-// on the current device (done at context creation, outside any capture).
+// Opts every core-kernel instantiation into its dynamic shared memory size on
+// the current device (done at context creation, outside any capture).
 int init_kernel_attrs(std::string* err) {
-#define AWC_ATTR(T, BY)                                                                    \
-  CUDA_TRY(err, cudaFuncSetAttribute(awc::step3d_tma<T, BY, kTmaStages>,                   \
+#define AWC_ATTR(T, TY)                                                                    \
+  CUDA_TRY(err, cudaFuncSetAttribute(awc::step3d_core<T, TY, stages<T>()>,                 \
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,          \
-                                     tma_smem<T, BY>()))
+                                     core_smem<T, TY>()))
+  AWC_ATTR(float, 2);
   AWC_ATTR(float, 4);
   AWC_ATTR(float, 8);
-  AWC_ATTR(float, 16);
+  AWC_ATTR(double, 2);
   AWC_ATTR(double, 4);
   AWC_ATTR(double, 8);
-  AWC_ATTR(double, 16);
 #undef AWC_ATTR
   return AWC_OK;
 }
 
-template <typename T, int BY>
-int launch_tma(awc_plan* P, int64_t it, const awc::StepParams<T>& S, dim3 grid, cudaStream_t st) {
-  awc::step3d_tma<T, BY, kTmaStages><<<grid, dim3(32, BY), tma_smem<T, BY>(), st>>>(
+template <typename T, int TY>
+void launch_core(awc_plan* P, int64_t it, const awc::StepParams<T>& S, dim3 grid, cudaStream_t st) {
+  awc::step3d_core<T, TY, stages<T>()><<<grid, dim3(32, TY), core_smem<T, TY>(), st>>>(
       P->map_c[(it + 1) % 3], P->map_o[it % 3], P->map_f, S);
-  return AWC_OK;
 }
 
+// One time step. 3D: the shell kernel on the context's second stream and the
+// core kernel on its main stream, forked from and joined back into the main
+// stream (parallel branches once captured in a graph). 2D: one kernel.
 template <typename T>
 int launch_step(awc_plan* P, int64_t it, cudaStream_t st) {
+  awc_ctx* C = P->ctx;
   const awc_problem* p = &P->p;
   awc::StepParams<T> S = step_params<T>(P, it);
-  const dim3 grid = step_grid(P);
-  int rc = AWC_OK;
-  if (p->ndim == 3 && P->kernel == 1) {
-    switch (P->by) {
-      case 4: rc = launch_tma<T, 4>(P, it, S, grid, st); break;
-      case 8: rc = launch_tma<T, 8>(P, it, S, grid, st); break;
-      case 16: rc = launch_tma<T, 16>(P, it, S, grid, st); break;
-      default: return set_err(&P->ctx->err, AWC_ERR_INVALID, "unsupported tile height %d", P->by);
-    }
-  } else if (p->ndim == 3) {
-    switch (P->by) {
-      case 4: awc::step3d<T, 4><<<grid, dim3(32, 4), 0, st>>>(S); break;
-      case 8: awc::step3d<T, 8><<<grid, dim3(32, 8), 0, st>>>(S); break;
-      case 16: awc::step3d<T, 16><<<grid, dim3(32, 16), 0, st>>>(S); break;
-      default: return set_err(&P->ctx->err, AWC_ERR_INVALID, "unsupported tile height %d", P->by);
-    }
+  if (p->ndim == 2) {
+    kernel_params(P, 0, S);
+    awc::step2d<T><<<step_grid(P), dim3(32, 8), 0, st>>>(S);
   } else {
-    awc::step2d<T><<<grid, dim3(32, 8), 0, st>>>(S);
+    const bool shell = P->nbox > 0, core = P->has_core;
+    if (shell && core) {
+      CUDA_TRY(&C->err, cudaEventRecord(C->ev_fork, st));
+      CUDA_TRY(&C->err, cudaStreamWaitEvent(C->stream2, C->ev_fork, 0));
+    }
+    if (shell) {
+      awc::StepParams<T> Sh = S;
+      kernel_params(P, 1, Sh);
+      awc::step3d_band<T><<<(unsigned)P->box_blk[P->nbox], dim3(32, 8), 0,
+                             core ? C->stream2 : st>>>(Sh);
+    }
+    if (core) {
+      kernel_params(P, 0, S);
+      const dim3 grid = step_grid(P);
+      switch (P->by) {
+        case 4: launch_core<T, 2>(P, it, S, grid, st); break;
+        case 8: launch_core<T, 4>(P, it, S, grid, st); break;
+        case 16: launch_core<T, 8>(P, it, S, grid, st); break;
+        default: return set_err(&C->err, AWC_ERR_INVALID, "unsupported tile height %d", P->by);
+      }
+    }
+    if (shell && core) {
+      CUDA_TRY(&C->err, cudaEventRecord(C->ev_join, C->stream2));
+      CUDA_TRY(&C->err, cudaStreamWaitEvent(st, C->ev_join, 0));
+    }
   }
-  if (rc) return rc;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
-    return set_err(&P->ctx->err, AWC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+    return set_err(&C->err, AWC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
   return AWC_OK;
 }
 
@@ -634,7 +775,7 @@ int launch_range(awc_plan* P, int64_t start, int64_t n, cudaStream_t st) {
 int prepare_launch(awc_plan* P) {
   int rc;
   if ((rc = ensure_io(P))) return rc;
-  if (P->p.ndim == 3 && P->kernel == 1 && (rc = ensure_maps(P))) return rc;
+  if (P->p.ndim == 3 && P->has_core && (rc = ensure_maps(P))) return rc;
   return AWC_OK;
 }
 
@@ -677,63 +818,44 @@ int get_graph(awc_plan* P, int64_t start, int64_t n, cudaGraphExec_t* out) {
   return AWC_OK;
 }
 
-int occupancy(const awc_plan* P, int kernel, int by) {
+int occupancy(const awc_plan* P, int by) {
   int occ = 0;
   const bool f64 = P->p.precision == AWC_F64;
-  auto reg = [&](auto fn) { cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * by, 0); };
-  auto tma = [&](auto fn, int smem) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 32 * by, smem);
-  };
-#define AWC_SMEM(T, BY) tma_smem<T, BY>()
-  if (kernel == 1) {
-    if (f64) {
-      if (by == 4) tma(awc::step3d_tma<double, 4, kTmaStages>, AWC_SMEM(double, 4));
-      if (by == 8) tma(awc::step3d_tma<double, 8, kTmaStages>, AWC_SMEM(double, 8));
-      if (by == 16) tma(awc::step3d_tma<double, 16, kTmaStages>, AWC_SMEM(double, 16));
-    } else {
-      if (by == 4) tma(awc::step3d_tma<float, 4, kTmaStages>, AWC_SMEM(float, 4));
-      if (by == 8) tma(awc::step3d_tma<float, 8, kTmaStages>, AWC_SMEM(float, 8));
-      if (by == 16) tma(awc::step3d_tma<float, 16, kTmaStages>, AWC_SMEM(float, 16));
-    }
+#define AWC_OCC(T, TY)                                                                     \
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, awc::step3d_core<T, TY, stages<T>()>, \
+                                                32 * TY, core_smem<T, TY>())
+  if (f64) {
+    if (by == 4) AWC_OCC(double, 2);
+    if (by == 8) AWC_OCC(double, 4);
+    if (by == 16) AWC_OCC(double, 8);
   } else {
-    if (f64) {
-      if (by == 4) reg(awc::step3d<double, 4>);
-      if (by == 8) reg(awc::step3d<double, 8>);
-      if (by == 16) reg(awc::step3d<double, 16>);
-    } else {
-      if (by == 4) reg(awc::step3d<float, 4>);
-      if (by == 8) reg(awc::step3d<float, 8>);
-      if (by == 16) reg(awc::step3d<float, 16>);
-    }
+    if (by == 4) AWC_OCC(float, 2);
+    if (by == 8) AWC_OCC(float, 4);
+    if (by == 16) AWC_OCC(float, 8);
   }
-#undef AWC_SMEM
+#undef AWC_OCC
   cudaGetLastError();
   return occ > 0 ? occ : 1;
 }
 
-// z chunk that spreads the tiles of one (kernel, tile height) over about
-// `waves` rounds of resident blocks.
-int32_t chunk_for(const awc_plan* P, int kernel, int by, double waves) {
-  const awc_problem* p = &P->p;
-  const int64_t iz = p->nz - 2;
-  const int64_t tiles = ((p->nx - 2) / 32 + 1) * ((p->ny - 2 + by - 1) / by);
-  const int64_t resident = (int64_t)P->ctx->num_sms * occupancy(P, kernel, by);
+// z chunk that spreads the core tiles of one tile height over about `waves`
+// rounds of resident blocks.
+int32_t chunk_for(const awc_plan* P, int by, double waves) {
+  if (!P->has_core) return 1;
+  const awc::Box& C = P->core;
+  const int64_t iz = C.z1 - C.z0 + 1;
+  const int64_t tiles = ((C.x1 - P->core_x) / 64 + 1) * ((C.y1 - C.y0 + by) / by);
+  const int64_t resident = (int64_t)P->ctx->num_sms * occupancy(P, by);
   int64_t nch = (int64_t)std::llround(waves * (double)resident / (double)std::max<int64_t>(tiles, 1));
   nch = std::max<int64_t>(1, std::min<int64_t>(nch, iz));
   return (int32_t)((iz + nch - 1) / nch);
 }
 
-// Default launch shape: 3D uses the TMA pipeline with 32 x 8 tiles and one
-// wave of resident blocks; the autotuner refines it.
+// Default launch shape: 64 x 8 core tiles and one wave of resident blocks;
+// the autotuner refines it.
 void default_tuning(awc_plan* P) {
   P->by = 8;
-  if (P->p.ndim != 3) {
-    P->kernel = 0;
-    P->zchunk = 1;
-    return;
-  }
-  P->kernel = tensor_map_encoder() ? 1 : 0;
-  P->zchunk = chunk_for(P, P->kernel, P->by, 1.0);
+  P->zchunk = P->p.ndim == 3 ? chunk_for(P, P->by, 1.0) : 1;
 }
 
 int forward_impl(awc_ctx* C, const awc_problem* p, const double* vel, const double* coeffs,
@@ -861,7 +983,10 @@ int awc_create(awc_ctx** out, int32_t device) {
   C->device = device;
   C->num_sms = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreate(&C->ev0) != cudaSuccess || cudaEventCreate(&C->ev1) != cudaSuccess) {
+      cudaStreamCreateWithFlags(&C->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&C->ev0) != cudaSuccess || cudaEventCreate(&C->ev1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&C->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&C->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     awc_destroy(C);
     return set_err(nullptr, AWC_ERR_CUDA, "stream/event creation failed");
   }
@@ -875,8 +1000,12 @@ void awc_destroy(awc_ctx* ctx) {
   for (awc_plan* P : ctx->cache) delete P;
   ctx->cache.clear();
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -994,71 +1123,95 @@ int awc_plan_field(awc_plan* P, double* out) {
   return AWC_OK;
 }
 
-int32_t awc_plan_launches_per_step(const awc_plan* P) { return P ? 1 : 0; }
+int32_t awc_plan_launches_per_step(const awc_plan* P) {
+  if (!P) return 0;
+  return (P->p.ndim == 3 && P->has_core && P->nbox > 0) ? 2 : 1;
+}
 
-int awc_plan_set_launch(awc_plan* P, int32_t kernel, int32_t tile_y, int32_t zchunk) {
+int awc_plan_set_launch(awc_plan* P, int32_t tile_y, int32_t zchunk, int32_t band_zchunk) {
   if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
-  if (kernel != 0 && kernel != 1) return set_err(&P->ctx->err, AWC_ERR_INVALID, "kernel must be 0 or 1");
-  if (kernel == 1 && !tensor_map_encoder())
-    return set_err(&P->ctx->err, AWC_ERR_INVALID, "the TMA kernel needs cuTensorMapEncodeTiled");
   if (tile_y != 4 && tile_y != 8 && tile_y != 16)
     return set_err(&P->ctx->err, AWC_ERR_INVALID, "tile_y must be 4, 8 or 16");
-  if (zchunk < 1) return set_err(&P->ctx->err, AWC_ERR_INVALID, "zchunk must be >= 1");
+  if (zchunk < 1 || band_zchunk < 1 || band_zchunk > 255)
+    return set_err(&P->ctx->err, AWC_ERR_INVALID, "zchunk must be >= 1, band_zchunk in [1, 255]");
   if (P->p.ndim == 3) {
-    P->kernel = kernel;
     P->by = tile_y;
     P->zchunk = (int32_t)std::min<int64_t>(zchunk, P->p.nz - 2);
+    P->szc = band_zchunk;
+    box_blocks(P);
   }
   return AWC_OK;
 }
 
-int awc_plan_get_launch(const awc_plan* P, int32_t* kernel, int32_t* tile_y, int32_t* zchunk) {
-  if (!P || !kernel || !tile_y || !zchunk) return set_err(nullptr, AWC_ERR_INVALID, "NULL argument");
-  *kernel = P->kernel;
+int awc_plan_get_launch(const awc_plan* P, int32_t* tile_y, int32_t* zchunk, int32_t* band_zchunk) {
+  if (!P || !tile_y || !zchunk || !band_zchunk)
+    return set_err(nullptr, AWC_ERR_INVALID, "NULL argument");
   *tile_y = P->by;
   *zchunk = P->zchunk;
+  *band_zchunk = P->szc;
   return AWC_OK;
 }
+
+namespace {
+// Device time per step [ms] of the current launch shape over n steps (the
+// state is reset before and is garbage after).
+int time_shape(awc_plan* P, int64_t n, float* per) {
+  int rc;
+  if ((rc = awc_plan_reset(P)) || (rc = awc_plan_run(P, 1, 0, nullptr))) return rc;  // warm-up
+  float ms = 0.f;
+  if ((rc = awc_plan_run(P, n, 0, &ms))) return rc;
+  *per = ms / (float)n;
+  return AWC_OK;
+}
+}  // namespace
 
 int awc_plan_autotune(awc_plan* P, int64_t steps, float* best_ms_per_step) {
   if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
   awc_ctx* C = P->ctx;
   if (steps < 1) return set_err(&C->err, AWC_ERR_INVALID, "steps must be >= 1");
-  if (P->p.ndim != 3 || P->p.nt < 1) {
+  if (P->p.ndim != 3 || P->p.nt < 2) {
     if (best_ms_per_step) *best_ms_per_step = 0.f;
     return AWC_OK;
   }
-  const int64_t n = std::min<int64_t>(steps, P->p.nt);
-  struct Cand { int32_t kernel, by, zchunk; };
-  std::vector<Cand> cands;
-  const int nk = tensor_map_encoder() ? 2 : 1;
-  for (int kernel = nk - 1; kernel >= 0; --kernel)
-    for (int by : {4, 8, 16})
-      for (double waves : {0.5, 1.0, 2.0, 4.0}) {
-        const Cand c{kernel, by, chunk_for(P, kernel, by, waves)};
-        bool dup = false;
-        for (const Cand& d : cands) dup = dup || (d.kernel == c.kernel && d.by == c.by && d.zchunk == c.zchunk);
-        if (!dup) cands.push_back(c);
-      }
-  float best = 1e30f;
-  Cand win = {P->kernel, P->by, P->zchunk};
+  const int64_t n = std::min<int64_t>(steps, P->p.nt - 1);
   int rc;
-  for (const Cand& c : cands) {
-    P->kernel = c.kernel;
-    P->by = c.by;
-    P->zchunk = c.zchunk;
-    if ((rc = awc_plan_reset(P)) || (rc = awc_plan_run(P, 1, 0, nullptr))) return rc;  // warm-up
-    float ms = 0.f;
-    if ((rc = awc_plan_run(P, n, 0, &ms))) return rc;
-    const float per = ms / (float)n;
+  // phase 1: core tile height and z chunk
+  std::vector<std::pair<int32_t, int32_t>> cands;
+  for (int by : {4, 8, 16})
+    for (double waves : {0.5, 1.0, 2.0, 4.0, 8.0}) {
+      const std::pair<int32_t, int32_t> c{by, chunk_for(P, by, waves)};
+      if (std::find(cands.begin(), cands.end(), c) == cands.end()) cands.push_back(c);
+    }
+  float best = 1e30f;
+  std::pair<int32_t, int32_t> win{P->by, P->zchunk};
+  for (const auto& c : cands) {
+    P->by = c.first;
+    P->zchunk = c.second;
+    float per = 0.f;
+    if ((rc = time_shape(P, n, &per))) return rc;
     if (per < best) {
       best = per;
       win = c;
     }
   }
-  P->kernel = win.kernel;
-  P->by = win.by;
-  P->zchunk = win.zchunk;
+  P->by = win.first;
+  P->zchunk = win.second;
+  // phase 2: z planes per block of the band kernel
+  if (P->nbox > 0) {
+    int32_t wz = P->szc;
+    for (int32_t zc : {5, 10, 20, 40}) {
+      P->szc = zc;
+      box_blocks(P);
+      float per = 0.f;
+      if ((rc = time_shape(P, n, &per))) return rc;
+      if (per < best) {
+        best = per;
+        wz = zc;
+      }
+    }
+    P->szc = wz;
+    box_blocks(P);
+  }
   if (best_ms_per_step) *best_ms_per_step = best;
   return awc_plan_reset(P);
 }

@@ -13,12 +13,14 @@
 //     are served by block 0 (nothing else writes the rim of pnew during a
 //     step, so this needs no ordering against the other blocks).
 //
-// Memory layout in HBM (x fastest, like the reference's column-major arrays):
-//   p fields, fact   pitched: node (i, j, k) at i + px*(j + ny*k), px = nx
-//                    rounded up to 32 elements (128/256-byte rows, so every
-//                    TMA stride and tile origin is 16-byte aligned)
-//   ψ axis x  (halo+1, ny, nz)   ψ axis y (nx, halo+1, nz)   ψ axis z (nx, ny, halo+1)
-//   ξ axis x  (halo,   ny, nz)   ξ axis y (nx, halo,   nz)   ξ axis z (nx, ny, halo)
+// Memory layout in HBM (x fastest, like the reference's column-major arrays;
+// px = nx rounded up to 32 elements, so rows are 128/256-byte aligned and
+// every TMA stride and tile origin is 16-byte aligned):
+//   p fields, fact   node (i, j, k) at i + px*(j + ny*k)
+//   ψ axis x  (halo+1, ny, nz)   q + (halo+1)*(j + ny*k)
+//   ψ axis y  (px, halo+1, nz)   i + px*(q + (halo+1)*k)
+//   ψ axis z  (px, ny, halo+1)   i + px*(j + ny*q)
+//   ξ         the same with halo entries and q-1 in place of q.
 // ψ is double-buffered (old/new): node c needs the new ψ on both of its
 // faces, ψ[q] (between c and c+1) and ψ[q-1] (between c-1 and c). Both depend
 // only on pcur and the old ψ, so each node recomputes the two values it needs
@@ -32,10 +34,6 @@
 // Left band: c <= halo, ψ index q = c. Right band: c >= n-halo-1 (and not in
 // the left band), q = c - (n-halo-2). ξ and on-grid coefficients use q-1,
 // half-grid coefficients use q and q-1.
-//
-// Tiles: a block owns x range [32 bx, 32 bx + 32) (nodes 0 and nx-1 are rim
-// and not computed), y range [1 + BY by, 1 + BY (by+1)) and, in 3D, z planes
-// [1 + zchunk bz, ...). Thread (tx, ty) owns node (32 bx + tx, 1 + BY by + ty).
 #pragma once
 #include <cstdint>
 #include <cuda.h>
@@ -55,8 +53,8 @@ struct BandSide {
 };
 
 // A node that carries sources and/or receivers. Interior entries are
-// bucketed by the block that owns the node: {local thread index in the
-// block, z plane (3D), source group, receiver group}; a group is an index
+// bucketed by the block that owns the node: {node index inside the block's
+// tile, z plane (3D), source group, receiver group}; a group is an index
 // into a CSR (off/ids) list, -1 when the node has none of that kind.
 struct IoRim {
   int64_t node;  // pitched linear index of a Dirichlet-rim node
@@ -78,6 +76,11 @@ struct Io {
   T* traces;               // [nt][nrec]
 };
 
+// Inclusive 0-based node ranges of an axis-aligned box.
+struct Box {
+  int32_t x0, x1, y0, y1, z0, z1;
+};
+
 template <typename T>
 struct StepParams {
   const T* pold;
@@ -85,53 +88,28 @@ struct StepParams {
   T* pnew;
   const T* fact;
   int32_t nx, ny, nz, halo;
-  int64_t px;              // row pitch of the fields (elements)
+  int64_t px;              // row pitch of fields and y/z band arrays (elements)
   T inv_d[3];
   T inv_d2[3];
   BandSide<T> band[3][2];  // [axis][left/right]
   int32_t active[3][2];    // side carries a non-trivial CPML recursion
   int32_t first_r[3];      // first node (0-based) of the right band per axis
-  int32_t zchunk;          // planes per block along z (3D)
+  int32_t zchunk;          // planes per block along z (3D core kernel)
   int32_t it;              // 0-based time step index (row of stf/traces)
   int32_t* err;            // set to 1 when a bounded device wait runs out
-  Io<T> io;
+  Io<T> io;                // this kernel's sources/receivers
+  int32_t do_rim;          // this kernel's block 0 serves the rim nodes
+  // 3D core kernel: the box of nodes outside every active CPML band, tiled
+  // from x = core_x (a 16-byte-aligned origin at or below core.x0)
+  Box core;
+  int32_t core_x;
+  // 3D shell kernel: disjoint boxes covering the interior nodes outside the
+  // core box; box b owns blocks [box_blk[b], box_blk[b+1])
+  int32_t nbox;
+  Box box[6];
+  int32_t box_blk[7];
+  int32_t shell_zchunk;  // planes per block of the band kernel
 };
-
-// ---------------------------------------------------------------------------
-// CPML band arithmetic, split into the loads (issued early) and the update.
-template <typename T>
-struct BandVals {
-  T pq, pm, xi;  // old ψ[q], old ψ[q-1], ξ[q-1]
-};
-
-template <typename T>
-__device__ __forceinline__ BandVals<T> band_load(const BandSide<T>& B, int q, int64_t psi_base,
-                                                 int64_t xi_base, int64_t stride) {
-  BandVals<T> v;
-  v.pq = B.psi_old[psi_base + (int64_t)q * stride];
-  v.pm = B.psi_old[psi_base + (int64_t)(q - 1) * stride];
-  v.xi = B.xi[xi_base + (int64_t)(q - 1) * stride];
-  return v;
-}
-
-// pm, pc, pp: pressure at c-1, c, c+1 along the axis; d2: that axis's second
-// difference; f: fact at the node.
-template <typename T>
-__device__ __forceinline__ void band_apply(const BandSide<T>& B, const BandVals<T>& L, int q,
-                                           bool first, T pm, T pc, T pp, T d2, T f, T inv_d,
-                                           int64_t psi_base, int64_t xi_base, int64_t stride,
-                                           T& damp) {
-  // update_ψ!: ψ = b_K_h ψ + a_h (p[c+1] - p[c]) / d, on both faces of the node
-  const T ps_q = B.bKh[q] * L.pq + B.ah[q] * (pp - pc) * inv_d;
-  const T ps_m = B.bKh[q - 1] * L.pm + B.ah[q - 1] * (pc - pm) * inv_d;
-  B.psi_new[psi_base + (int64_t)q * stride] = ps_q;
-  if (first) B.psi_new[psi_base + (int64_t)(q - 1) * stride] = ps_m;
-  // update_p! band branch: dψ, ξ recursion, damping term
-  const T dpsi = (ps_q - ps_m) * inv_d;
-  const T xn = B.bK[q - 1] * L.xi + B.a[q - 1] * (d2 + dpsi);
-  B.xi[xi_base + (int64_t)(q - 1) * stride] = xn;
-  damp += f * (dpsi + xn);
-}
 
 // Which band (if any) coordinate c of an axis of length n lies in.
 // Returns 0 none, 1 left, 2 right; sets q and `first`.
@@ -149,22 +127,26 @@ __device__ __forceinline__ int band_of(int c, int n, int halo, int first_r, int&
   return 0;
 }
 
-// Element offsets of a node's band entries: ψ at psi_base + q*stride, ξ at
-// xi_base + (q-1)*stride, for the three axes.
-struct BandAddr {
-  int64_t psi_base, xi_base, stride;
-};
-__device__ __forceinline__ BandAddr addr_x(int halo, int ny, int j, int k) {
-  const int64_t jk = (int64_t)j + (int64_t)ny * k;
-  return {(int64_t)(halo + 1) * jk, (int64_t)halo * jk, 1};
-}
-__device__ __forceinline__ BandAddr addr_y(int halo, int nx, int i, int k) {
-  return {(int64_t)i + (int64_t)nx * (halo + 1) * k, (int64_t)i + (int64_t)nx * halo * k,
-          (int64_t)nx};
-}
-__device__ __forceinline__ BandAddr addr_z(int nx, int ny, int i, int j) {
-  const int64_t c = (int64_t)i + (int64_t)nx * j;
-  return {c, c, (int64_t)nx * ny};
+// One axis of the CPML band update at one node: ψ on both faces (update_ψ!),
+// dψ, the ξ recursion and the damping term (update_p! band branch).
+// ψ entry q sits at psi_base + q*stride, ξ entry q-1 at xi_base + (q-1)*stride.
+// pm, pc, pp: pressure at c-1, c, c+1 along the axis; d2: that axis's second
+// difference; f: fact at the node.
+template <typename T>
+__device__ __forceinline__ void band_axis(const BandSide<T>& B, int q, bool first, T pm, T pc,
+                                          T pp, T d2, T f, T inv_d, int64_t psi_base,
+                                          int64_t xi_base, int64_t stride, T& damp) {
+  const T ps_q_old = B.psi_old[psi_base + (int64_t)q * stride];
+  const T ps_m_old = B.psi_old[psi_base + (int64_t)(q - 1) * stride];
+  const T ps_q = B.bKh[q] * ps_q_old + B.ah[q] * (pp - pc) * inv_d;
+  const T ps_m = B.bKh[q - 1] * ps_m_old + B.ah[q - 1] * (pc - pm) * inv_d;
+  B.psi_new[psi_base + (int64_t)q * stride] = ps_q;
+  if (first) B.psi_new[psi_base + (int64_t)(q - 1) * stride] = ps_m;
+  const T dpsi = (ps_q - ps_m) * inv_d;
+  T* xp = B.xi + xi_base + (int64_t)(q - 1) * stride;
+  const T xn = B.bK[q - 1] * (*xp) + B.a[q - 1] * (d2 + dpsi);
+  *xp = xn;
+  damp += f * (dpsi + xn);
 }
 
 // Sources then receivers of one node, for the thread that owns its value v.
@@ -192,140 +174,6 @@ __device__ __forceinline__ void rim_io(const Io<T>& io, T* pnew, int it) {
   }
 }
 
-// Walks this block's source/receiver entries of plane k (sorted by plane).
-template <typename T>
-__device__ __forceinline__ T plane_io(const Io<T>& io, int it, int& e, int e1, int k, int local,
-                                      bool valid, T v) {
-  for (; e < e1; ++e) {
-    const int4 en = io.ent[e];
-    if (en.y != k) break;
-    if (valid && en.x == local) v = node_io(io, it, en.z, en.w, v);
-  }
-  return v;
-}
-
-// ---------------------------------------------------------------------------
-// 3D step, register-queue variant: 2.5D blocking with the current plane of
-// pcur (and a one-node ring) in shared memory for the x/y neighbours and the
-// z neighbours in registers; the next plane's loads are issued one iteration
-// ahead.
-template <typename T, int BY>
-__global__ void __launch_bounds__(32 * BY) step3d(StepParams<T> P) {
-  __shared__ T tile[BY + 2][32 + 2];
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int nx = P.nx, ny = P.ny, nz = P.nz, halo = P.halo;
-  const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-  if (blk == 0 && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
-  const int i = blockIdx.x * 32 + tx;
-  const int j = 1 + blockIdx.y * BY + ty;
-  const bool valid = i >= 1 && i <= nx - 2 && j <= ny - 2;
-  const int k0 = 1 + blockIdx.z * P.zchunk;
-  int k1 = k0 + P.zchunk;
-  if (k1 > nz - 1) k1 = nz - 1;
-  if (k0 >= k1) return;  // block-uniform
-
-  const int64_t px = P.px;
-  const int64_t plane = px * ny;
-  const int64_t col = (int64_t)i + px * j;
-  const bool ldxl = valid && (tx == 0 || i == 1);
-  const bool ldxr = valid && (tx == 31 || i == nx - 2);
-  const bool ldyl = valid && ty == 0;
-  const bool ldyh = valid && (ty == BY - 1 || j == ny - 2);
-
-  const T* __restrict__ pcur = P.pcur;
-  T pm = 0, pc = 0, pp = 0, po = 0, f = 0;
-  T rxl = 0, rxr = 0, ryl = 0, ryh = 0;
-  if (valid) {
-    const int64_t o0 = col + (int64_t)k0 * plane;
-    pm = __ldg(pcur + o0 - plane);
-    pc = __ldg(pcur + o0);
-    pp = __ldg(pcur + o0 + plane);
-    po = __ldg(P.pold + o0);
-    f = __ldg(P.fact + o0);
-    if (ldxl) rxl = __ldg(pcur + o0 - 1);
-    if (ldxr) rxr = __ldg(pcur + o0 + 1);
-    if (ldyl) ryl = __ldg(pcur + o0 - px);
-    if (ldyh) ryh = __ldg(pcur + o0 + px);
-  }
-  int qx = 0, qy = 0;
-  bool fx = false, fy = false;
-  const int bx = valid ? band_of(i, nx, halo, P.first_r[0], qx, fx) : 0;
-  const int by = valid ? band_of(j, ny, halo, P.first_r[1], qy, fy) : 0;
-  const bool doxb = bx != 0 && P.active[0][bx - 1];
-  const bool doyb = by != 0 && P.active[1][by - 1];
-  int ioe = P.io.blk_off[blk];
-  const int ioe1 = P.io.blk_off[blk + 1];
-  const int local = tx + 32 * ty;
-
-  for (int k = k0; k < k1; ++k) {
-    const int64_t o = col + (int64_t)k * plane;
-    T npp = 0, npo = 0, nf = 0, nxl = 0, nxr = 0, nyl = 0, nyh = 0;
-    if (valid && k + 1 < k1) {
-      const int64_t on = o + plane;
-      npp = __ldg(pcur + on + plane);
-      npo = __ldg(P.pold + on);
-      nf = __ldg(P.fact + on);
-      if (ldxl) nxl = __ldg(pcur + on - 1);
-      if (ldxr) nxr = __ldg(pcur + on + 1);
-      if (ldyl) nyl = __ldg(pcur + on - px);
-      if (ldyh) nyh = __ldg(pcur + on + px);
-    }
-    __syncthreads();  // the previous plane's readers are done with the tile
-    if (valid) {
-      tile[ty + 1][tx + 1] = pc;
-      if (ldxl) tile[ty + 1][tx] = rxl;
-      if (ldxr) tile[ty + 1][tx + 2] = rxr;
-      if (ldyl) tile[ty][tx + 1] = ryl;
-      if (ldyh) tile[ty + 2][tx + 1] = ryh;
-    }
-    __syncthreads();
-    T v = 0;
-    if (valid) {
-      const T xm = tile[ty + 1][tx], xp = tile[ty + 1][tx + 2];
-      const T ym = tile[ty][tx + 1], yp = tile[ty + 2][tx + 1];
-      const T d2x = (xp - T(2) * pc + xm) * P.inv_d2[0];
-      const T d2y = (yp - T(2) * pc + ym) * P.inv_d2[1];
-      const T d2z = (pp - T(2) * pc + pm) * P.inv_d2[2];
-      T damp = 0;
-      if (doxb) {
-        const BandAddr a = addr_x(halo, ny, j, k);
-        const BandSide<T>& B = P.band[0][bx - 1];
-        band_apply(B, band_load(B, qx, a.psi_base, a.xi_base, a.stride), qx, fx, xm, pc, xp, d2x,
-                   f, P.inv_d[0], a.psi_base, a.xi_base, a.stride, damp);
-      }
-      if (doyb) {
-        const BandAddr a = addr_y(halo, nx, i, k);
-        const BandSide<T>& B = P.band[1][by - 1];
-        band_apply(B, band_load(B, qy, a.psi_base, a.xi_base, a.stride), qy, fy, ym, pc, yp, d2y,
-                   f, P.inv_d[1], a.psi_base, a.xi_base, a.stride, damp);
-      }
-      {
-        int qz;
-        bool fz;
-        const int bz = band_of(k, nz, halo, P.first_r[2], qz, fz);
-        if (bz != 0 && P.active[2][bz - 1]) {
-          const BandAddr a = addr_z(nx, ny, i, j);
-          const BandSide<T>& B = P.band[2][bz - 1];
-          band_apply(B, band_load(B, qz, a.psi_base, a.xi_base, a.stride), qz, fz, pm, pc, pp,
-                     d2z, f, P.inv_d[2], a.psi_base, a.xi_base, a.stride, damp);
-        }
-      }
-      v = T(2) * pc - po + f * (d2x + d2y + d2z) + damp;
-    }
-    v = plane_io(P.io, P.it, ioe, ioe1, k, local, valid, v);
-    if (valid) P.pnew[o] = v;
-    pm = pc;
-    pc = pp;
-    pp = npp;
-    po = npo;
-    f = nf;
-    rxl = nxl;
-    rxr = nxr;
-    ryl = nyl;
-    ryh = nyh;
-  }
-}
-
 // ---------------------------------------------------------------------------
 // TMA / mbarrier primitives (sm_90+ PTX, used here on sm_100a).
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -342,20 +190,28 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// One try_wait with a suspend-time hint: the warp sleeps in hardware until the
+// phase completes or about `ns` nanoseconds pass, instead of spinning.
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity, uint32_t ns) {
   uint32_t ok;
   asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
       : "memory");
   return ok != 0;
 }
-// Bounded wait on a phase of an mbarrier: false when the limit runs out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int n = 0; n < (1 << 22); ++n)
-    if (mbar_try_wait(bar, parity)) return true;
+// Bounded wait on a phase: at most ~4 s (4096 x 1 ms), or until another thread
+// of the block has raised `abort`. False when it gives up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  for (int n = 0; n < 4096; ++n) {
+    if (mbar_try_wait(bar, parity, 1000000u)) return true;
+    if (*abort) return false;
+  }
   return false;
 }
 // 3D tiled TMA load of one box into shared memory, completing on `bar`.
@@ -368,51 +224,101 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
-// Shared-memory layout of one pipeline stage (plane m) of step3d_tma.
-template <typename T, int BY>
-struct TmaStage {
-  static constexpr int A = 16 / (int)sizeof(T);  // x apron keeping the box origin 16-B aligned
-  static constexpr int PW = 32 + 2 * A;          // pcur box width
-  static constexpr int PC_BYTES = PW * (BY + 2) * (int)sizeof(T);
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+
+// Geometry of the 3D step kernel for element type T and TY thread rows:
+// a block of 32 x TY threads owns a 64 x 2TY tile of (x, y) nodes; thread
+// (tx, ty) owns the 2 x 2 nodes x0 + 2tx + {0,1}, y0 + 2ty + {0,1}. One
+// pipeline stage holds, for one z plane, the pcur box (64 + 2A) x (2TY + 2)
+// around the tile (x apron A keeps the box origin 16-byte aligned; the y ring
+// is one row) and the pold and fact boxes 64 x 2TY.
+template <typename T, int TY>
+struct Tile3 {
+  static constexpr int TX = 64;
+  static constexpr int RY = 2 * TY;
+  static constexpr int A = 16 / (int)sizeof(T);
+  static constexpr int PW = TX + 2 * A;
+  static constexpr int PC_BYTES = PW * (RY + 2) * (int)sizeof(T);
   static constexpr int PC_PAD = (PC_BYTES + 127) / 128 * 128;
-  static constexpr int IN_BYTES = 32 * BY * (int)sizeof(T);
+  static constexpr int IN_BYTES = TX * RY * (int)sizeof(T);
   static constexpr int BYTES = PC_PAD + 2 * IN_BYTES;
 };
 
+// CPML band work of one node: every active band axis the node lies in.
+template <typename T>
+__device__ __forceinline__ T band_node(const StepParams<T>& P, int i, int j, int k, T pc, T xm,
+                                       T xp, T ym, T yp, T pm, T pp, T d2x, T d2y, T d2z, T f) {
+  T damp = 0;
+  int q;
+  bool first;
+  const int bx = band_of(i, P.nx, P.halo, P.first_r[0], q, first);
+  if (bx != 0 && P.active[0][bx - 1]) {
+    const int64_t jk = (int64_t)j + (int64_t)P.ny * k;
+    band_axis(P.band[0][bx - 1], q, first, xm, pc, xp, d2x, f, P.inv_d[0],
+              (int64_t)(P.halo + 1) * jk, (int64_t)P.halo * jk, (int64_t)1, damp);
+  }
+  const int by = band_of(j, P.ny, P.halo, P.first_r[1], q, first);
+  if (by != 0 && P.active[1][by - 1]) {
+    band_axis(P.band[1][by - 1], q, first, ym, pc, yp, d2y, f, P.inv_d[1],
+              (int64_t)i + P.px * (P.halo + 1) * k, (int64_t)i + P.px * P.halo * k, P.px, damp);
+  }
+  const int bz = band_of(k, P.nz, P.halo, P.first_r[2], q, first);
+  if (bz != 0 && P.active[2][bz - 1]) {
+    const int64_t c = (int64_t)i + P.px * j;
+    band_axis(P.band[2][bz - 1], q, first, pm, pc, pp, d2z, f, P.inv_d[2], c, c, P.px * P.ny,
+              damp);
+  }
+  return damp;
+}
+
 // ---------------------------------------------------------------------------
-// 3D step, TMA-pipelined variant. Same tile/chunk decomposition as step3d;
-// one elected thread streams, per z plane m, three boxes into a ring of S
-// shared-memory stages with cp.async.bulk.tensor:
-//   pcur (32 + 2A) x (BY + 2) around the tile (the x/y ring included;
-//        outside the grid TMA fills zeros), pold 32 x BY, fact 32 x BY,
-// each stage completing on its own mbarrier. Plane k is computed from the
-// stages of planes k-1, k, k+1 while the loads of planes up to k+S-2 are in
-// flight, so the memory pipeline runs S-3 planes ahead with no register cost.
-// The CPML band values of the plane are loaded by the owning threads before
-// they wait on the plane's barrier.
-template <typename T, int BY, int S>
-__global__ void __launch_bounds__(32 * BY) step3d_tma(const __grid_constant__ CUtensorMap mc,
-                                                      const __grid_constant__ CUtensorMap mo,
-                                                      const __grid_constant__ CUtensorMap mf,
-                                                      StepParams<T> P) {
-  using L = TmaStage<T, BY>;
+// 3D core step: the nodes of P.core, which lie outside every active CPML
+// band, so no band state is touched. Grid: x tiles of 64 nodes from P.core_x,
+// y tiles of 2TY rows from core.y0, z chunks of `zchunk` planes from core.z0.
+// One elected thread streams the planes of the block's chunk through S
+// shared-memory stages with cp.async.bulk.tensor, each stage with a "full"
+// mbarrier (TMA bytes) and an "empty" mbarrier (one arrival per warp once the
+// warp is done with the stage). Plane k is computed from the stages of planes
+// k-1, k, k+1; loads run up to S-3 planes ahead and warps may drift apart by
+// as much, with no block-wide barrier in the loop. Each thread owns 2 x 2
+// nodes: an x pair read and written as one vector, in two rows.
+template <typename T, int TY, int S>
+__global__ void __launch_bounds__(32 * TY) step3d_core(const __grid_constant__ CUtensorMap mc,
+                                                       const __grid_constant__ CUtensorMap mo,
+                                                       const __grid_constant__ CUtensorMap mf,
+                                                       StepParams<T> P) {
+  using L = Tile3<T, TY>;
+  using V2 = typename Vec2<T>::type;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S * L::BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * L::BYTES);
+  uint64_t* empty = full + S;
+  volatile int* abort = reinterpret_cast<volatile int*>(empty + S);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
-  const int nx = P.nx, ny = P.ny, nz = P.nz, halo = P.halo;
   const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-  if (blk == 0 && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
-  const int x0 = blockIdx.x * 32, y0 = 1 + blockIdx.y * BY;
-  const int i = x0 + tx, j = y0 + ty;
-  const bool valid = i >= 1 && i <= nx - 2 && j <= ny - 2;
-  const int k0 = 1 + blockIdx.z * P.zchunk;
+  if (blk == 0 && P.do_rim && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
+  const Box C = P.core;
+  const int x0 = P.core_x + blockIdx.x * L::TX, y0 = C.y0 + blockIdx.y * L::RY;
+  const int k0 = C.z0 + blockIdx.z * P.zchunk;
   int k1 = k0 + P.zchunk;
-  if (k1 > nz - 1) k1 = nz - 1;
+  if (k1 > C.z1 + 1) k1 = C.z1 + 1;
   if (k0 >= k1) return;  // block-uniform
   const int nplanes = k1 - k0 + 2;  // pcur planes k0-1 .. k1
 
   if (tid == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], TY);
+    }
+    *abort = 0;
     fence_mbar_init();
   }
   __syncthreads();
@@ -420,93 +326,307 @@ __global__ void __launch_bounds__(32 * BY) step3d_tma(const __grid_constant__ CU
   auto issue = [&](int u) {
     const int s = u % S, m = k0 - 1 + u;
     unsigned char* st = smem + s * L::BYTES;
-    const bool full = m >= k0 && m < k1;
-    mbar_expect_tx(&bar[s], L::PC_BYTES + (full ? 2 * L::IN_BYTES : 0));
-    tma_load_3d(st, &mc, &bar[s], x0 - L::A, y0 - 1, m);
-    if (full) {
-      tma_load_3d(st + L::PC_PAD, &mo, &bar[s], x0, y0, m);
-      tma_load_3d(st + L::PC_PAD + L::IN_BYTES, &mf, &bar[s], x0, y0, m);
+    const bool inner = m >= k0 && m < k1;
+    mbar_expect_tx(&full[s], L::PC_BYTES + (inner ? 2 * L::IN_BYTES : 0));
+    tma_load_3d(st, &mc, &full[s], x0 - L::A, y0 - 1, m);
+    if (inner) {
+      tma_load_3d(st + L::PC_PAD, &mo, &full[s], x0, y0, m);
+      tma_load_3d(st + L::PC_PAD + L::IN_BYTES, &mf, &full[s], x0, y0, m);
     }
   };
   if (tid == 0)
     for (int u = 0; u < S && u < nplanes; ++u) issue(u);
 
-  int qx = 0, qy = 0;
-  bool fx = false, fy = false;
-  const int bx = valid ? band_of(i, nx, halo, P.first_r[0], qx, fx) : 0;
-  const int by = valid ? band_of(j, ny, halo, P.first_r[1], qy, fy) : 0;
-  const bool doxb = bx != 0 && P.active[0][bx - 1];
-  const bool doyb = by != 0 && P.active[1][by - 1];
+  // the thread's 2 x 2 nodes
+  const int xa = x0 + 2 * tx, j0 = y0 + 2 * ty;
+  const bool vx0 = xa >= C.x0 && xa <= C.x1, vx1 = xa + 1 >= C.x0 && xa + 1 <= C.x1;
+  const bool vy0 = j0 <= C.y1, vy1 = j0 + 1 <= C.y1;
+  const bool any = (vx0 || vx1) && vy0;
+  const bool all4 = vx0 && vx1 && vy0 && vy1;
+  const int64_t px = P.px, plane = px * P.ny;
+  int64_t o = (int64_t)xa + px * j0 + plane * k0;  // pitched offset of node (xa, j0, k)
   int ioe = P.io.blk_off[blk];
   const int ioe1 = P.io.blk_off[blk + 1];
-  const int64_t px = P.px, plane = px * ny;
-  const int64_t col = (int64_t)i + px * j;
-  constexpr int A = L::A, PW = L::PW;
+  const int c0 = (2 * ty + 1) * L::PW + 2 * tx + L::A;  // pcur stage index of (xa, j0)
+  const int i0 = 2 * ty * L::TX + 2 * tx;               // pold/fact stage index of (xa, j0)
+  const T ix2 = P.inv_d2[0], iy2 = P.inv_d2[1], iz2 = P.inv_d2[2];
 
-  bool ok = mbar_wait(&bar[0], 0) && mbar_wait(&bar[1 % S], (1 / S) & 1);
+  bool ok = mbar_wait(&full[0], 0, abort) && mbar_wait(&full[1 % S], (1 / S) & 1, abort);
   int uc = 1;  // use index of the current plane
-  for (int k = k0; k < k1; ++k, ++uc) {
-    // CPML band values of this plane, issued before the barrier wait
-    BandVals<T> lx{}, ly{}, lz{};
-    int qz = 0;
-    bool fz = false;
-    const int bz = band_of(k, nz, halo, P.first_r[2], qz, fz);
-    const bool dozb = valid && bz != 0 && P.active[2][bz - 1];
-    const BandAddr axx = addr_x(halo, ny, j, k), ayy = addr_y(halo, nx, i, k),
-                   azz = addr_z(nx, ny, i, j);
-    if (doxb) lx = band_load(P.band[0][bx - 1], qx, axx.psi_base, axx.xi_base, axx.stride);
-    if (doyb) ly = band_load(P.band[1][by - 1], qy, ayy.psi_base, ayy.xi_base, ayy.stride);
-    if (dozb) lz = band_load(P.band[2][bz - 1], qz, azz.psi_base, azz.xi_base, azz.stride);
-
-    ok = ok && mbar_wait(&bar[(uc + 1) % S], ((uc + 1) / S) & 1);
+  for (int k = k0; k < k1; ++k, ++uc, o += plane) {
+    ok = ok && mbar_wait(&full[(uc + 1) % S], ((uc + 1) / S) & 1, abort);
+    if (!ok) break;
     const T* cm = reinterpret_cast<const T*>(smem + ((uc - 1) % S) * L::BYTES);
     const T* cc = reinterpret_cast<const T*>(smem + (uc % S) * L::BYTES);
     const T* cp = reinterpret_cast<const T*>(smem + ((uc + 1) % S) * L::BYTES);
     const T* oo = reinterpret_cast<const T*>(smem + (uc % S) * L::BYTES + L::PC_PAD);
-    const T* ff = oo + 32 * BY;
+    const T* ff = oo + L::TX * L::RY;
+    // rows j0 and j0+1: centre pairs, x apron scalars, y and z neighbours,
+    // pold and fact
+    const V2 c_0 = *reinterpret_cast<const V2*>(cc + c0);
+    const V2 c_1 = *reinterpret_cast<const V2*>(cc + c0 + L::PW);
+    const T xm0 = cc[c0 - 1], xp0 = cc[c0 + 2], xm1 = cc[c0 + L::PW - 1], xp1 = cc[c0 + L::PW + 2];
+    const V2 ym = *reinterpret_cast<const V2*>(cc + c0 - L::PW);
+    const V2 yp = *reinterpret_cast<const V2*>(cc + c0 + 2 * L::PW);
+    const V2 zm0 = *reinterpret_cast<const V2*>(cm + c0);
+    const V2 zm1 = *reinterpret_cast<const V2*>(cm + c0 + L::PW);
+    const V2 zp0 = *reinterpret_cast<const V2*>(cp + c0);
+    const V2 zp1 = *reinterpret_cast<const V2*>(cp + c0 + L::PW);
+    const V2 po0 = *reinterpret_cast<const V2*>(oo + i0);
+    const V2 po1 = *reinterpret_cast<const V2*>(oo + i0 + L::TX);
+    const V2 f_0 = *reinterpret_cast<const V2*>(ff + i0);
+    const V2 f_1 = *reinterpret_cast<const V2*>(ff + i0 + L::TX);
+    // node (row, x): 2 pcur - pold + fact * (d2x + d2y + d2z)
+    T v00 = T(2) * c_0.x - po0.x +
+            f_0.x * ((c_0.y - T(2) * c_0.x + xm0) * ix2 + (c_1.x - T(2) * c_0.x + ym.x) * iy2 +
+                     (zp0.x - T(2) * c_0.x + zm0.x) * iz2);
+    T v01 = T(2) * c_0.y - po0.y +
+            f_0.y * ((xp0 - T(2) * c_0.y + c_0.x) * ix2 + (c_1.y - T(2) * c_0.y + ym.y) * iy2 +
+                     (zp0.y - T(2) * c_0.y + zm0.y) * iz2);
+    T v10 = T(2) * c_1.x - po1.x +
+            f_1.x * ((c_1.y - T(2) * c_1.x + xm1) * ix2 + (yp.x - T(2) * c_1.x + c_0.x) * iy2 +
+                     (zp1.x - T(2) * c_1.x + zm1.x) * iz2);
+    T v11 = T(2) * c_1.y - po1.y +
+            f_1.y * ((xp1 - T(2) * c_1.y + c_1.x) * ix2 + (yp.y - T(2) * c_1.y + c_0.y) * iy2 +
+                     (zp1.y - T(2) * c_1.y + zm1.y) * iz2);
+    // sources and receivers of this plane (block-uniform walk, rarely taken)
+    for (; ioe < ioe1; ++ioe) {
+      const int4 en = P.io.ent[ioe];
+      if (en.y != k) break;
+      const int lx = en.x & (L::TX - 1), ly = en.x / L::TX;
+      if ((lx >> 1) == tx && (ly >> 1) == ty) {
+        const int sub = ((ly & 1) << 1) | (lx & 1);
+        if (sub == 0) v00 = node_io(P.io, P.it, en.z, en.w, v00);
+        if (sub == 1) v01 = node_io(P.io, P.it, en.z, en.w, v01);
+        if (sub == 2) v10 = node_io(P.io, P.it, en.z, en.w, v10);
+        if (sub == 3) v11 = node_io(P.io, P.it, en.z, en.w, v11);
+      }
+    }
+    // this warp is done with stage uc-1; the producer may refill it
+    __syncwarp();
+    if (tx == 0) mbar_arrive(&empty[(uc - 1) % S]);
+    if (all4) {
+      *reinterpret_cast<V2*>(P.pnew + o) = V2{v00, v01};
+      *reinterpret_cast<V2*>(P.pnew + o + px) = V2{v10, v11};
+    } else if (any) {
+      if (vx0) P.pnew[o] = v00;
+      if (vx1) P.pnew[o + 1] = v01;
+      if (vy1 && vx0) P.pnew[o + px] = v10;
+      if (vy1 && vx1) P.pnew[o + px + 1] = v11;
+    }
+    if (tid == 0 && uc - 1 + S < nplanes) {
+      if (!mbar_wait(&empty[(uc - 1) % S], ((uc - 1) / S) & 1, abort)) {
+        ok = false;
+        break;
+      }
+      issue(uc - 1 + S);
+    }
+  }
+  if (!ok) {
+    // a wait ran out: record it, stop the block, and let the producer drain
+    // the loads it still has in flight before the block's memory goes away
+    *abort = 1;
+    atomicExch(P.err, 1);
+    if (tid == 0) {
+      const int issued = nplanes < uc - 1 + S ? nplanes : uc - 1 + S;
+      for (int u = uc; u < issued; ++u) {
+        for (int n = 0; n < 64; ++n)
+          if (mbar_try_wait(&full[u % S], (u / S) & 1, 1000000u)) break;
+      }
+    }
+  }
+}
+
+// One side of one band axis as seen by a fixed node column: the node's
+// ψ/ξ entries and coefficients (q fixed for x and y bands along z).
+template <typename T>
+struct AxisCol {
+  const T* pold;  // old ψ at entry q of the current plane
+  T* pnew;        // new ψ at entry q
+  T* xi;          // ξ at entry q-1
+  int64_t dpsi, dxi;     // element offset of ψ[q-1] from ψ[q]; of ξ to the next plane
+  int64_t step_psi;      // ψ offset to the next plane
+  T ahq, ahm, bkhq, bkhm, a1, bk1;  // a_h[q], a_h[q-1], bK_h[q], bK_h[q-1], a[q-1], bK[q-1]
+  bool first;
+};
+
+template <typename T>
+__device__ __forceinline__ void axis_col_init(AxisCol<T>& A, const BandSide<T>& B, int q,
+                                              bool first, int64_t psi_off, int64_t xi_off,
+                                              int64_t qstride, int64_t step_psi,
+                                              int64_t step_xi) {
+  A.pold = B.psi_old + psi_off + (int64_t)q * qstride;
+  A.pnew = B.psi_new + psi_off + (int64_t)q * qstride;
+  A.xi = B.xi + xi_off + (int64_t)(q - 1) * qstride;
+  A.dpsi = qstride;
+  A.dxi = step_xi;
+  A.step_psi = step_psi;
+  A.ahq = B.ah[q];
+  A.ahm = B.ah[q - 1];
+  A.bkhq = B.bKh[q];
+  A.bkhm = B.bKh[q - 1];
+  A.a1 = B.a[q - 1];
+  A.bk1 = B.bK[q - 1];
+  A.first = first;
+}
+
+// ---------------------------------------------------------------------------
+// 3D band step: the interior nodes outside P.core (the CPML bands), in the
+// boxes P.box[0..nbox). A block of 32 x 8 threads owns a 32 x 8 column tile
+// of a box and streams `zchunk`-plane chunks of it (P.shell_zchunk); each
+// thread keeps its column's z neighbours in registers, and its x and y band
+// state (entry pointers and coefficients, fixed along z) in registers. The
+// z band, uniform over a plane, is looked up per plane.
+template <typename T>
+__global__ void __launch_bounds__(256) step3d_band(StepParams<T> P) {
+  const int blk = blockIdx.x;
+  if (blk == 0 && P.do_rim && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
+  int b = 0;
+  while (b + 1 < P.nbox && blk >= P.box_blk[b + 1]) ++b;
+  const Box B = P.box[b];
+  const int zc = P.shell_zchunk;
+  int r = blk - P.box_blk[b];
+  const int gx = (B.x1 - B.x0 + 32) / 32, gy = (B.y1 - B.y0 + 8) / 8;
+  const int tbx = r % gx;
+  r /= gx;
+  const int tby = r % gy;
+  const int k0 = B.z0 + (r / gy) * zc;
+  const int k1 = min(k0 + zc, B.z1 + 1);
+  const int i = B.x0 + tbx * 32 + threadIdx.x, j = B.y0 + tby * 8 + threadIdx.y;
+  const bool valid = i <= B.x1 && j <= B.y1;
+  const int nx = P.nx, ny = P.ny, nz = P.nz, halo = P.halo;
+  const int64_t px = P.px, plane = px * ny;
+  int64_t o = (int64_t)i + px * j + plane * k0;
+  int ioe = P.io.blk_off[blk];
+  const int ioe1 = P.io.blk_off[blk + 1];
+  const int local = threadIdx.x + 32 * threadIdx.y;
+  // x and y band state of the column
+  AxisCol<T> ax{}, ay{};
+  bool dox = false, doy = false;
+  if (valid) {
+    int q;
+    bool first;
+    const int sx = band_of(i, nx, halo, P.first_r[0], q, first);
+    if (sx != 0 && P.active[0][sx - 1]) {
+      const int64_t jk = (int64_t)j + (int64_t)ny * k0;
+      axis_col_init(ax, P.band[0][sx - 1], q, first, (int64_t)(halo + 1) * jk,
+                    (int64_t)halo * jk, (int64_t)1, (int64_t)(halo + 1) * ny,
+                    (int64_t)halo * ny);
+      dox = true;
+    }
+    const int sy = band_of(j, ny, halo, P.first_r[1], q, first);
+    if (sy != 0 && P.active[1][sy - 1]) {
+      axis_col_init(ay, P.band[1][sy - 1], q, first, (int64_t)i + px * (halo + 1) * k0,
+                    (int64_t)i + px * halo * k0, px, px * (halo + 1), px * halo);
+      doy = true;
+    }
+  }
+  const T* __restrict__ pcur = P.pcur;
+  T pm = 0, pc = 0, pp = 0;
+  if (valid) {
+    pm = __ldg(pcur + o - plane);
+    pc = __ldg(pcur + o);
+  }
+  const int64_t col = (int64_t)i + px * j;
+  for (int k = k0; k < k1; ++k, o += plane) {
     T v = 0;
-    if (valid && ok) {
-      const int c = (ty + 1) * PW + tx + A;
-      const T pc = cc[c], xm = cc[c - 1], xp = cc[c + 1], ym = cc[c - PW], yp = cc[c + PW];
-      const T pm = cm[c], pp = cp[c];
-      const T po = oo[ty * 32 + tx], f = ff[ty * 32 + tx];
+    if (valid) {
+      pp = __ldg(pcur + o + plane);
+      const T xm = __ldg(pcur + o - 1), xp = __ldg(pcur + o + 1);
+      const T ym = __ldg(pcur + o - px), yp = __ldg(pcur + o + px);
+      const T po = __ldg(P.pold + o), f = __ldg(P.fact + o);
+      // band values of this plane, issued before the arithmetic
+      T xq = 0, xmq = 0, xx = 0, yq = 0, ymq = 0, yx = 0, zq = 0, zmq = 0, zx = 0;
+      if (dox) {
+        xq = ax.pold[0];
+        xmq = ax.pold[-ax.dpsi];
+        xx = ax.xi[0];
+      }
+      if (doy) {
+        yq = ay.pold[0];
+        ymq = ay.pold[-ay.dpsi];
+        yx = ay.xi[0];
+      }
+      int qz;
+      bool fz;
+      const int sz = band_of(k, nz, halo, P.first_r[2], qz, fz);
+      const bool doz = sz != 0 && P.active[2][sz - 1];
+      const BandSide<T>& BZ = P.band[2][sz > 0 ? sz - 1 : 0];
+      if (doz) {
+        zq = BZ.psi_old[col + plane * qz];
+        zmq = BZ.psi_old[col + plane * (qz - 1)];
+        zx = BZ.xi[col + plane * (qz - 1)];
+      }
       const T d2x = (xp - T(2) * pc + xm) * P.inv_d2[0];
       const T d2y = (yp - T(2) * pc + ym) * P.inv_d2[1];
       const T d2z = (pp - T(2) * pc + pm) * P.inv_d2[2];
+      v = T(2) * pc - po + f * (d2x + d2y + d2z);
       T damp = 0;
-      if (doxb)
-        band_apply(P.band[0][bx - 1], lx, qx, fx, xm, pc, xp, d2x, f, P.inv_d[0], axx.psi_base,
-                   axx.xi_base, axx.stride, damp);
-      if (doyb)
-        band_apply(P.band[1][by - 1], ly, qy, fy, ym, pc, yp, d2y, f, P.inv_d[1], ayy.psi_base,
-                   ayy.xi_base, ayy.stride, damp);
-      if (dozb)
-        band_apply(P.band[2][bz - 1], lz, qz, fz, pm, pc, pp, d2z, f, P.inv_d[2], azz.psi_base,
-                   azz.xi_base, azz.stride, damp);
-      v = T(2) * pc - po + f * (d2x + d2y + d2z) + damp;
-    }
-    v = plane_io(P.io, P.it, ioe, ioe1, k, tid, valid && ok, v);
-    if (valid && ok) P.pnew[col + (int64_t)k * plane] = v;
-    // every thread is done with stage (uc-1): refill it with plane use uc-1+S
-    if (__syncthreads_or(!ok)) {
-      // a wait ran out: record it and drain what this block still has in flight
-      if (tid == 0) {
-        atomicExch(P.err, 1);
-        for (int u = uc + 1; u < nplanes && u < uc - 1 + S; ++u) mbar_wait(&bar[u % S], (u / S) & 1);
+      if (dox) {  // update_ψ_x! and the x branch of update_p!
+        const T inv = P.inv_d[0];
+        const T sq = ax.bkhq * xq + ax.ahq * (xp - pc) * inv;
+        const T sm = ax.bkhm * xmq + ax.ahm * (pc - xm) * inv;
+        ax.pnew[0] = sq;
+        if (ax.first) ax.pnew[-ax.dpsi] = sm;
+        const T dps = (sq - sm) * inv;
+        const T xn = ax.bk1 * xx + ax.a1 * (d2x + dps);
+        ax.xi[0] = xn;
+        damp += f * (dps + xn);
       }
-      return;
+      if (doy) {
+        const T inv = P.inv_d[1];
+        const T sq = ay.bkhq * yq + ay.ahq * (yp - pc) * inv;
+        const T sm = ay.bkhm * ymq + ay.ahm * (pc - ym) * inv;
+        ay.pnew[0] = sq;
+        if (ay.first) ay.pnew[-ay.dpsi] = sm;
+        const T dps = (sq - sm) * inv;
+        const T xn = ay.bk1 * yx + ay.a1 * (d2y + dps);
+        ay.xi[0] = xn;
+        damp += f * (dps + xn);
+      }
+      if (doz) {
+        const T inv = P.inv_d[2];
+        const T sq = BZ.bKh[qz] * zq + BZ.ah[qz] * (pp - pc) * inv;
+        const T sm = BZ.bKh[qz - 1] * zmq + BZ.ah[qz - 1] * (pc - pm) * inv;
+        BZ.psi_new[col + plane * qz] = sq;
+        if (fz) BZ.psi_new[col + plane * (qz - 1)] = sm;
+        const T dps = (sq - sm) * inv;
+        const T xn = BZ.bK[qz - 1] * zx + BZ.a[qz - 1] * (d2z + dps);
+        BZ.xi[col + plane * (qz - 1)] = xn;
+        damp += f * (dps + xn);
+      }
+      v += damp;
     }
-    if (tid == 0 && uc - 1 + S < nplanes) issue(uc - 1 + S);
+    // sources and receivers of this plane (block-uniform walk)
+    for (; ioe < ioe1; ++ioe) {
+      const int4 en = P.io.ent[ioe];
+      if (en.y != k) break;
+      if (valid && en.x == local) v = node_io(P.io, P.it, en.z, en.w, v);
+    }
+    if (valid) P.pnew[o] = v;
+    pm = pc;
+    pc = pp;
+    if (dox) {
+      ax.pold += ax.step_psi;
+      ax.pnew += ax.step_psi;
+      ax.xi += ax.dxi;
+    }
+    if (doy) {
+      ay.pold += ay.step_psi;
+      ay.pnew += ay.step_psi;
+      ay.xi += ay.dxi;
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
-// 2D step: one thread per interior node; neighbours through L1.
+// 2D step: one thread per interior node (x tiles of 32 from x = 0, y tiles of
+// 8 rows from y = 1); neighbours through L1.
 template <typename T>
 __global__ void __launch_bounds__(256) step2d(StepParams<T> P) {
   const int nx = P.nx, ny = P.ny, halo = P.halo;
   const int blk = blockIdx.x + gridDim.x * blockIdx.y;
-  if (blk == 0 && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
+  if (blk == 0 && P.do_rim && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
   const int i = blockIdx.x * 32 + threadIdx.x;
   const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   if (i < 1 || i > nx - 2 || j > ny - 2) return;
@@ -523,18 +643,13 @@ __global__ void __launch_bounds__(256) step2d(StepParams<T> P) {
   int q;
   bool first;
   const int bx = band_of(i, nx, halo, P.first_r[0], q, first);
-  if (bx != 0 && P.active[0][bx - 1]) {
-    const BandSide<T>& B = P.band[0][bx - 1];
-    const int64_t pb = (int64_t)(halo + 1) * j, xb = (int64_t)halo * j;
-    band_apply(B, band_load(B, q, pb, xb, (int64_t)1), q, first, xm, pc, xp, d2x, f, P.inv_d[0],
-               pb, xb, (int64_t)1, damp);
-  }
+  if (bx != 0 && P.active[0][bx - 1])
+    band_axis(P.band[0][bx - 1], q, first, xm, pc, xp, d2x, f, P.inv_d[0],
+              (int64_t)(halo + 1) * j, (int64_t)halo * j, (int64_t)1, damp);
   const int by = band_of(j, ny, halo, P.first_r[1], q, first);
-  if (by != 0 && P.active[1][by - 1]) {
-    const BandSide<T>& B = P.band[1][by - 1];
-    band_apply(B, band_load(B, q, (int64_t)i, (int64_t)i, (int64_t)nx), q, first, ym, pc, yp, d2y,
-               f, P.inv_d[1], (int64_t)i, (int64_t)i, (int64_t)nx, damp);
-  }
+  if (by != 0 && P.active[1][by - 1])
+    band_axis(P.band[1][by - 1], q, first, ym, pc, yp, d2y, f, P.inv_d[1], (int64_t)i,
+              (int64_t)i, px, damp);
   T v = T(2) * pc - po + f * (d2x + d2y) + damp;
   const int local = threadIdx.x + 32 * threadIdx.y;
   for (int e = P.io.blk_off[blk]; e < P.io.blk_off[blk + 1]; ++e) {

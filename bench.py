@@ -46,6 +46,8 @@ def parse_args():
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
     ap.add_argument("--quick", action="store_true",
                     help="device-resident leg only (no e2e, FP64 or CPU legs); for profiling")
+    ap.add_argument("--launch", default=None,
+                    help="tile_y,zchunk,band_zchunk of the 3D step instead of autotuning")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the CPU-baseline sample")
     return ap.parse_args()
@@ -261,7 +263,10 @@ def main():
 
     # ---- device-resident leg ------------------------------------------------
     plan = ctx.plan(p, s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"], s["posrecs"])
-    plan.autotune(20)  # launch shape picked on this data, before any timing
+    if args.launch:
+        plan.set_launch(*[int(x) for x in args.launch.split(",")])
+    else:
+        plan.autotune(20)  # launch shape picked on this data, before any timing
     launch = plan.get_launch()
 
     def shot():
@@ -297,8 +302,8 @@ def main():
                          f"{p.nx * p.ny * p.nz * (4 if args.precision == 'f32' else 8) / 1e6:.1f}"
                          " MB each, no flush needed)",
                    "parallelism": f"shots{world}",
-                   "launch": {"kernel": ["register-queue", "tma-pipeline"][launch[0]],
-                              "tile": [32, launch[1]], "zchunk": launch[2]}},
+                   "launch": {"core_tile": [64, launch[0]], "core_zchunk": launch[1],
+                              "band_zchunk": launch[2]}},
         "gcells_per_s": world * interior_cells(p) / t_ts / 1e9,
         "us_per_timestep": t_ts * 1e6,
         "a_eff_bytes_per_timestep": ab,

@@ -142,16 +142,18 @@ int64_t awc_plan_step(const awc_plan* plan);
  * and the current field (the latest new pressure, nx*ny*nz) to the host. */
 int awc_plan_traces(awc_plan* plan, double* traces);
 int awc_plan_field(awc_plan* plan, double* p);
-/* Number of kernel launches one time step issues (for launch accounting). */
+/* Number of kernel launches one time step issues (for launch accounting):
+ * 2 for a 3D problem with both a core and a CPML band region, else 1. */
 int32_t awc_plan_launches_per_step(const awc_plan* plan);
-/* Launch shape of the 3D step kernel. kernel 0 keeps the z neighbours in a
- * register queue; kernel 1 streams z planes through a TMA + mbarrier pipeline
- * in shared memory. `tile_y` rows (4, 8 or 16) of 32-wide x tiles per block
- * and `zchunk` z planes streamed per block (>= 1). Every shape gives the
- * same results; only the speed differs. The state is kept. 2D plans ignore
- * the call. */
-int awc_plan_set_launch(awc_plan* plan, int32_t kernel, int32_t tile_y, int32_t zchunk);
-int awc_plan_get_launch(const awc_plan* plan, int32_t* kernel, int32_t* tile_y, int32_t* zchunk);
+/* Launch shape of a 3D time step, which runs as two kernels over disjoint
+ * nodes: the core kernel (nodes outside every CPML band; blocks of 64 x
+ * `tile_y` nodes, tile_y = 4, 8 or 16, streaming `zchunk` z planes through a
+ * TMA pipeline) and the band kernel (the CPML band nodes; 32 x 8 columns
+ * streaming `band_zchunk` planes, 1..255). Every shape gives the same
+ * results; only the speed differs. The state is kept. 2D plans ignore it. */
+int awc_plan_set_launch(awc_plan* plan, int32_t tile_y, int32_t zchunk, int32_t band_zchunk);
+int awc_plan_get_launch(const awc_plan* plan, int32_t* tile_y, int32_t* zchunk,
+                        int32_t* band_zchunk);
 /* Times `steps` time steps of every candidate launch shape on this plan's own
  * data, keeps the fastest, and resets the state. Writes the best time per
  * step [ms] to best_ms_per_step when not NULL. */

@@ -197,10 +197,9 @@ def test_launch_shapes_give_identical_results(pkg, ctx):
         plan.run()
         ref_t, ref_p = plan.traces(), plan.field()
         assert np.abs(ref_t).max() > 0
-        shapes = [(k, ty, zc) for k in (0, 1)
-                  for ty, zc in ((4, 1), (4, 7), (8, 3), (16, 5), (16, 100), (8, 26))]
-        for kn, ty, zc in shapes:
-            plan.set_launch(kn, ty, zc)
+        shapes = ((4, 1, 1), (4, 7, 3), (8, 3, 10), (16, 5, 255), (16, 100, 7), (8, 26, 2))
+        for ty, zc, bz in shapes:
+            plan.set_launch(ty, zc, bz)
             plan.reset()
             plan.run()
             np.testing.assert_array_equal(plan.traces(), ref_t)
@@ -220,8 +219,8 @@ def test_autotune_keeps_results(pkg, ctx):
     ref = plan.traces()
     best = plan.autotune(5)
     assert best > 0 and plan.step == 0
-    kn, ty, zc = plan.get_launch()
-    assert kn in (0, 1) and ty in (4, 8, 16) and zc >= 1
+    ty, zc, bz = plan.get_launch()
+    assert ty in (4, 8, 16) and zc >= 1 and bz >= 1
     plan.run()
     np.testing.assert_array_equal(plan.traces(), ref)
     plan.close()
