@@ -437,37 +437,20 @@ __global__ void __launch_bounds__(32 * TY) step3d_core(const __grid_constant__ C
   }
 }
 
-// One side of one band axis as seen by a fixed node column: the node's
-// ψ/ξ entries and coefficients (q fixed for x and y bands along z).
+// CPML update of one band axis at one node whose ψ entry q sits at element
+// `pq` of the side's arrays (ψ[q-1] at pq - dq) and ξ entry q-1 at `xq`.
 template <typename T>
-struct AxisCol {
-  const T* pold;  // old ψ at entry q of the current plane
-  T* pnew;        // new ψ at entry q
-  T* xi;          // ξ at entry q-1
-  int64_t dpsi, dxi;     // element offset of ψ[q-1] from ψ[q]; of ξ to the next plane
-  int64_t step_psi;      // ψ offset to the next plane
-  T ahq, ahm, bkhq, bkhm, a1, bk1;  // a_h[q], a_h[q-1], bK_h[q], bK_h[q-1], a[q-1], bK[q-1]
-  bool first;
-};
-
-template <typename T>
-__device__ __forceinline__ void axis_col_init(AxisCol<T>& A, const BandSide<T>& B, int q,
-                                              bool first, int64_t psi_off, int64_t xi_off,
-                                              int64_t qstride, int64_t step_psi,
-                                              int64_t step_xi) {
-  A.pold = B.psi_old + psi_off + (int64_t)q * qstride;
-  A.pnew = B.psi_new + psi_off + (int64_t)q * qstride;
-  A.xi = B.xi + xi_off + (int64_t)(q - 1) * qstride;
-  A.dpsi = qstride;
-  A.dxi = step_xi;
-  A.step_psi = step_psi;
-  A.ahq = B.ah[q];
-  A.ahm = B.ah[q - 1];
-  A.bkhq = B.bKh[q];
-  A.bkhm = B.bKh[q - 1];
-  A.a1 = B.a[q - 1];
-  A.bk1 = B.bK[q - 1];
-  A.first = first;
+__device__ __forceinline__ void band_apply(const BandSide<T>& B, int q, bool first, int64_t pq,
+                                           int64_t dq, int64_t xq, T psq, T psm, T xo, T pm,
+                                           T pc, T pp, T d2, T f, T inv, T& damp) {
+  const T sq = __ldg(B.bKh + q) * psq + __ldg(B.ah + q) * (pp - pc) * inv;
+  const T sm = __ldg(B.bKh + q - 1) * psm + __ldg(B.ah + q - 1) * (pc - pm) * inv;
+  B.psi_new[pq] = sq;
+  if (first) B.psi_new[pq - dq] = sm;
+  const T dps = (sq - sm) * inv;
+  const T xn = __ldg(B.bK + q - 1) * xo + __ldg(B.a + q - 1) * (d2 + dps);
+  B.xi[xq] = xn;
+  damp += f * (dps + xn);
 }
 
 // ---------------------------------------------------------------------------
@@ -500,27 +483,24 @@ __global__ void __launch_bounds__(256) step3d_band(StepParams<T> P) {
   int ioe = P.io.blk_off[blk];
   const int ioe1 = P.io.blk_off[blk + 1];
   const int local = threadIdx.x + 32 * threadIdx.y;
-  // x and y band state of the column
-  AxisCol<T> ax{}, ay{};
-  bool dox = false, doy = false;
+  // x and y band of the column (fixed along z): side, entry q, first flag,
+  // and the element offsets of ψ[q] and ξ[q-1] at the current plane
+  int sx = 0, sy = 0, qx = 0, qy = 0;
+  bool fx = false, fy = false;
+  int64_t pqx = 0, xqx = 0, pqy = 0, xqy = 0;
   if (valid) {
-    int q;
-    bool first;
-    const int sx = band_of(i, nx, halo, P.first_r[0], q, first);
-    if (sx != 0 && P.active[0][sx - 1]) {
-      const int64_t jk = (int64_t)j + (int64_t)ny * k0;
-      axis_col_init(ax, P.band[0][sx - 1], q, first, (int64_t)(halo + 1) * jk,
-                    (int64_t)halo * jk, (int64_t)1, (int64_t)(halo + 1) * ny,
-                    (int64_t)halo * ny);
-      dox = true;
-    }
-    const int sy = band_of(j, ny, halo, P.first_r[1], q, first);
-    if (sy != 0 && P.active[1][sy - 1]) {
-      axis_col_init(ay, P.band[1][sy - 1], q, first, (int64_t)i + px * (halo + 1) * k0,
-                    (int64_t)i + px * halo * k0, px, px * (halo + 1), px * halo);
-      doy = true;
-    }
+    sx = band_of(i, nx, halo, P.first_r[0], qx, fx);
+    if (sx != 0 && !P.active[0][sx - 1]) sx = 0;
+    sy = band_of(j, ny, halo, P.first_r[1], qy, fy);
+    if (sy != 0 && !P.active[1][sy - 1]) sy = 0;
+    const int64_t jk = (int64_t)j + (int64_t)ny * k0;
+    pqx = (int64_t)(halo + 1) * jk + qx;
+    xqx = (int64_t)halo * jk + (qx - 1);
+    pqy = (int64_t)i + px * (qy + (int64_t)(halo + 1) * k0);
+    xqy = (int64_t)i + px * ((qy - 1) + (int64_t)halo * k0);
   }
+  const int64_t stx_p = (int64_t)(halo + 1) * ny, stx_x = (int64_t)halo * ny;
+  const int64_t sty_p = px * (halo + 1), sty_x = px * halo;
   const T* __restrict__ pcur = P.pcur;
   T pm = 0, pc = 0, pp = 0;
   if (valid) {
@@ -528,73 +508,52 @@ __global__ void __launch_bounds__(256) step3d_band(StepParams<T> P) {
     pc = __ldg(pcur + o);
   }
   const int64_t col = (int64_t)i + px * j;
-  for (int k = k0; k < k1; ++k, o += plane) {
+  for (int k = k0; k < k1; ++k, o += plane, pqx += stx_p, xqx += stx_x, pqy += sty_p,
+           xqy += sty_x) {
     T v = 0;
     if (valid) {
       pp = __ldg(pcur + o + plane);
-      const T xm = __ldg(pcur + o - 1), xp = __ldg(pcur + o + 1);
-      const T ym = __ldg(pcur + o - px), yp = __ldg(pcur + o + px);
       const T po = __ldg(P.pold + o), f = __ldg(P.fact + o);
       // band values of this plane, issued before the arithmetic
       T xq = 0, xmq = 0, xx = 0, yq = 0, ymq = 0, yx = 0, zq = 0, zmq = 0, zx = 0;
-      if (dox) {
-        xq = ax.pold[0];
-        xmq = ax.pold[-ax.dpsi];
-        xx = ax.xi[0];
+      if (sx) {
+        const BandSide<T>& B = P.band[0][sx - 1];
+        xq = B.psi_old[pqx];
+        xmq = B.psi_old[pqx - 1];
+        xx = B.xi[xqx];
       }
-      if (doy) {
-        yq = ay.pold[0];
-        ymq = ay.pold[-ay.dpsi];
-        yx = ay.xi[0];
+      if (sy) {
+        const BandSide<T>& B = P.band[1][sy - 1];
+        yq = B.psi_old[pqy];
+        ymq = B.psi_old[pqy - px];
+        yx = B.xi[xqy];
       }
       int qz;
       bool fz;
-      const int sz = band_of(k, nz, halo, P.first_r[2], qz, fz);
-      const bool doz = sz != 0 && P.active[2][sz - 1];
-      const BandSide<T>& BZ = P.band[2][sz > 0 ? sz - 1 : 0];
-      if (doz) {
-        zq = BZ.psi_old[col + plane * qz];
-        zmq = BZ.psi_old[col + plane * (qz - 1)];
-        zx = BZ.xi[col + plane * (qz - 1)];
+      int sz = band_of(k, nz, halo, P.first_r[2], qz, fz);
+      if (sz != 0 && !P.active[2][sz - 1]) sz = 0;
+      if (sz) {
+        const BandSide<T>& B = P.band[2][sz - 1];
+        zq = B.psi_old[col + plane * qz];
+        zmq = B.psi_old[col + plane * (qz - 1)];
+        zx = B.xi[col + plane * (qz - 1)];
       }
+      const T xm = __ldg(pcur + o - 1), xp = __ldg(pcur + o + 1);
+      const T ym = __ldg(pcur + o - px), yp = __ldg(pcur + o + px);
       const T d2x = (xp - T(2) * pc + xm) * P.inv_d2[0];
       const T d2y = (yp - T(2) * pc + ym) * P.inv_d2[1];
       const T d2z = (pp - T(2) * pc + pm) * P.inv_d2[2];
       v = T(2) * pc - po + f * (d2x + d2y + d2z);
       T damp = 0;
-      if (dox) {  // update_ψ_x! and the x branch of update_p!
-        const T inv = P.inv_d[0];
-        const T sq = ax.bkhq * xq + ax.ahq * (xp - pc) * inv;
-        const T sm = ax.bkhm * xmq + ax.ahm * (pc - xm) * inv;
-        ax.pnew[0] = sq;
-        if (ax.first) ax.pnew[-ax.dpsi] = sm;
-        const T dps = (sq - sm) * inv;
-        const T xn = ax.bk1 * xx + ax.a1 * (d2x + dps);
-        ax.xi[0] = xn;
-        damp += f * (dps + xn);
-      }
-      if (doy) {
-        const T inv = P.inv_d[1];
-        const T sq = ay.bkhq * yq + ay.ahq * (yp - pc) * inv;
-        const T sm = ay.bkhm * ymq + ay.ahm * (pc - ym) * inv;
-        ay.pnew[0] = sq;
-        if (ay.first) ay.pnew[-ay.dpsi] = sm;
-        const T dps = (sq - sm) * inv;
-        const T xn = ay.bk1 * yx + ay.a1 * (d2y + dps);
-        ay.xi[0] = xn;
-        damp += f * (dps + xn);
-      }
-      if (doz) {
-        const T inv = P.inv_d[2];
-        const T sq = BZ.bKh[qz] * zq + BZ.ah[qz] * (pp - pc) * inv;
-        const T sm = BZ.bKh[qz - 1] * zmq + BZ.ah[qz - 1] * (pc - pm) * inv;
-        BZ.psi_new[col + plane * qz] = sq;
-        if (fz) BZ.psi_new[col + plane * (qz - 1)] = sm;
-        const T dps = (sq - sm) * inv;
-        const T xn = BZ.bK[qz - 1] * zx + BZ.a[qz - 1] * (d2z + dps);
-        BZ.xi[col + plane * (qz - 1)] = xn;
-        damp += f * (dps + xn);
-      }
+      if (sx)
+        band_apply(P.band[0][sx - 1], qx, fx, pqx, (int64_t)1, xqx, xq, xmq, xx, xm, pc, xp, d2x,
+                   f, P.inv_d[0], damp);
+      if (sy)
+        band_apply(P.band[1][sy - 1], qy, fy, pqy, px, xqy, yq, ymq, yx, ym, pc, yp, d2y, f,
+                   P.inv_d[1], damp);
+      if (sz)
+        band_apply(P.band[2][sz - 1], qz, fz, col + plane * qz, plane, col + plane * (qz - 1), zq,
+                   zmq, zx, pm, pc, pp, d2z, f, P.inv_d[2], damp);
       v += damp;
     }
     // sources and receivers of this plane (block-uniform walk)
@@ -606,16 +565,6 @@ __global__ void __launch_bounds__(256) step3d_band(StepParams<T> P) {
     if (valid) P.pnew[o] = v;
     pm = pc;
     pc = pp;
-    if (dox) {
-      ax.pold += ax.step_psi;
-      ax.pnew += ax.step_psi;
-      ax.xi += ax.dxi;
-    }
-    if (doy) {
-      ay.pold += ay.step_psi;
-      ay.pnew += ay.step_psi;
-      ay.xi += ay.dxi;
-    }
   }
 }
 
