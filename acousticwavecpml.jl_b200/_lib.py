@@ -95,6 +95,7 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32)]),
     "awc_plan_autotune": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_float)]),
+    "awc_forward2d_f32_static": (ctypes.c_int, [_PP, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _LIB = None

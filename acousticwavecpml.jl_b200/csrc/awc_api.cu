@@ -904,6 +904,12 @@ int check_device_flag(awc_plan* P) {
 
 }  // namespace
 
+namespace awc {
+// Sets the calling thread's last error (awc_last_error(NULL)) for entry
+// points defined in other translation units.
+void record_error(const char* msg) { g_thread_err = msg; }
+}  // namespace awc
+
 // ---------------------------------------------------------------------------
 extern "C" {
 

@@ -159,6 +159,30 @@ int awc_plan_get_launch(const awc_plan* plan, int32_t* tile_y, int32_t* zchunk,
  * step [ms] to best_ms_per_step when not NULL. */
 int awc_plan_autotune(awc_plan* plan, int64_t steps, float* best_ms_per_step);
 
+/* awc_forward for 2D FP32 problems without any device memory allocation.
+ * No counterpart in the reference (its solvers always allocate).
+ *
+ * For callers that cannot let a library call cudaMalloc: a solver loop that
+ * must not stall the device (cudaMalloc/cudaFree synchronise it), or a host
+ * framework whose own allocator owns all device memory (Julia CUDA.jl's pool,
+ * a caching allocator), where allocations it does not see starve it.
+ * Arguments, layouts and results are those of awc_forward with p->ndim == 2
+ * and p->precision == AWC_F32; no context is needed. Every device buffer of
+ * the solve lives in one fixed 32 MiB array of device memory, which exists on
+ * every GPU that loads this library until the process exits. A problem needs
+ * about 24 nx ny + 8 nt nrec + 8 nt nsrc bytes plus the CPML band arrays;
+ * larger problems are rejected with AWC_ERR_INVALID and a message giving the
+ * size needed (use awc_forward for them).
+ * The first call on each device looks up the array's device address; make
+ * that first call before any stream capture. Every call clears the state it
+ * needs, but all calls share the one array: calls that overlap on the GPU
+ * (from several host threads on one device) race and must be serialised by
+ * the caller. Runs on the current device and the legacy default stream and
+ * returns when the results are on the host. */
+int awc_forward2d_f32_static(const awc_problem* p, const double* vel, const double* coeffs,
+                             const int64_t* possrcs, const double* dt2srctf,
+                             const int64_t* posrecs, double* traces, double* pfinal);
+
 #ifdef __cplusplus
 }
 #endif
