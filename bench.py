@@ -266,7 +266,7 @@ def main():
     if args.launch:
         plan.set_launch(*[int(x) for x in args.launch.split(",")])
     else:
-        plan.autotune(20)  # launch shape picked on this data, before any timing
+        plan.autotune(40)  # launch shape picked on this data, before any timing
     launch = plan.get_launch()
 
     def shot():
