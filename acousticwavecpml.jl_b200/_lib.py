@@ -49,6 +49,20 @@ class Problem(ctypes.Structure):
     ]
 
 
+class Shot(ctypes.Structure):
+    """`awc_shot` of include/awcpml.h."""
+
+    _fields_ = [
+        ("model", ctypes.c_int32),
+        ("nsrc", ctypes.c_int32),
+        ("nrec", ctypes.c_int32),
+        ("coeffs", ctypes.c_void_p),
+        ("possrcs", ctypes.c_void_p),
+        ("dt2srctf", ctypes.c_void_p),
+        ("posrecs", ctypes.c_void_p),
+    ]
+
+
 class AwcError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{_ERRNAMES.get(code, 'error')} ({code}): {msg}")
@@ -96,6 +110,21 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_int32)]),
     "awc_plan_autotune": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_float)]),
     "awc_forward2d_f32_static": (ctypes.c_int, [_PP, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "awc_batch_create": (ctypes.c_int, [_vp, ctypes.c_int32, _PP, _vp, ctypes.c_int32, _vp,
+                                        ctypes.POINTER(_vp)]),
+    "awc_batch_destroy": (None, [_vp]),
+    "awc_batch_reset": (ctypes.c_int, [_vp]),
+    "awc_batch_run": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int32,
+                                     ctypes.POINTER(ctypes.c_float)]),
+    "awc_batch_step": (ctypes.c_int64, [_vp]),
+    "awc_batch_traces": (ctypes.c_int, [_vp, ctypes.c_int32, _vp]),
+    "awc_batch_field": (ctypes.c_int, [_vp, ctypes.c_int32, _vp]),
+    "awc_batch_set_launch": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32]),
+    "awc_batch_get_launch": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_int32)]),
+    "awc_batch_autotune": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_float)]),
+    "awc_forward_batch": (ctypes.c_int, [_vp, ctypes.c_int32, _PP, _vp, ctypes.c_int32, _vp,
+                                         _vp]),
 }
 
 _LIB = None

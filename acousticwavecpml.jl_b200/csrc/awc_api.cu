@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "../../include/awcpml.h"
+#include "awc_ctx.h"
 #include "awc_kernels.cuh"
 
 namespace {
@@ -161,19 +162,6 @@ template <typename T>
 constexpr int stages() { return sizeof(T) == 4 ? 6 : 4; }
 
 }  // namespace
-
-struct awc_ctx {
-  int device = 0;
-  int num_sms = 0;
-  cudaStream_t stream = nullptr;
-  cudaStream_t stream2 = nullptr;  // second branch of a 3D step (the shell kernel)
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  std::string err;
-  float last_run_ms = 0.f;
-  int64_t autotune_steps = 10;   // per candidate, for new 3D plans of awc_forward
-  std::vector<awc_plan*> cache;  // plans reused by awc_forward, most recent last
-};
 
 struct awc_plan {
   awc_ctx* ctx = nullptr;
@@ -908,6 +896,10 @@ namespace awc {
 // Sets the calling thread's last error (awc_last_error(NULL)) for entry
 // points defined in other translation units.
 void record_error(const char* msg) { g_thread_err = msg; }
+
+int fail(awc_ctx* ctx, int code, const char* msg) {
+  return set_err(ctx ? &ctx->err : nullptr, code, "%s", msg);
+}
 }  // namespace awc
 
 // ---------------------------------------------------------------------------

@@ -111,6 +111,22 @@ struct StepParams {
   int32_t shell_zchunk;  // planes per block of the band kernel
 };
 
+// The 2D node update with its rounding pinned, so that every 2D kernel (one
+// shot, batched shots, either path of the batched kernel) gives bitwise the
+// same value: each second difference is rounded on its own (a multiply the
+// compiler may not fuse into the following add), then the leapfrog is one
+// fused multiply-add, 2 pc - po + f (d2x + d2y).
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+template <typename T>
+__device__ __forceinline__ T second_diff(T m, T c, T p, T inv_d2) {
+  return mul_rn(p - T(2) * c + m, inv_d2);
+}
+template <typename T>
+__device__ __forceinline__ T leapfrog2d(T pc, T po, T f, T d2x, T d2y) {
+  return fma(f, d2x + d2y, T(2) * pc - po);
+}
+
 // Which band (if any) coordinate c of an axis of length n lies in.
 // Returns 0 none, 1 left, 2 right; sets q and `first`.
 __device__ __forceinline__ int band_of(int c, int n, int halo, int first_r, int& q, bool& first) {
@@ -586,8 +602,8 @@ __global__ void __launch_bounds__(256) step2d(StepParams<T> P) {
   const T xm = __ldg(pcur + o - 1), xp = __ldg(pcur + o + 1);
   const T ym = __ldg(pcur + o - px), yp = __ldg(pcur + o + px);
   const T po = __ldg(P.pold + o), f = __ldg(P.fact + o);
-  const T d2x = (xp - T(2) * pc + xm) * P.inv_d2[0];
-  const T d2y = (yp - T(2) * pc + ym) * P.inv_d2[1];
+  const T d2x = second_diff(xm, pc, xp, P.inv_d2[0]);
+  const T d2y = second_diff(ym, pc, yp, P.inv_d2[1]);
   T damp = 0;
   int q;
   bool first;
@@ -599,13 +615,149 @@ __global__ void __launch_bounds__(256) step2d(StepParams<T> P) {
   if (by != 0 && P.active[1][by - 1])
     band_axis(P.band[1][by - 1], q, first, ym, pc, yp, d2y, f, P.inv_d[1], (int64_t)i,
               (int64_t)i, px, damp);
-  T v = T(2) * pc - po + f * (d2x + d2y) + damp;
+  T v = leapfrog2d(pc, po, f, d2x, d2y) + damp;
   const int local = threadIdx.x + 32 * threadIdx.y;
   for (int e = P.io.blk_off[blk]; e < P.io.blk_off[blk + 1]; ++e) {
     const int4 en = P.io.ent[e];
     if (en.x == local) v = node_io(P.io, P.it, en.z, en.w, v);
   }
   P.pnew[o] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Batched 2D shots. Every shot owns its fields, CPML state, traces and
+// source/receiver lists; shots of one velocity model share fact. One launch
+// advances every shot of the batch by one time step: a persistent grid walks
+// the global list of 32 x (TY*R) tiles of all shots (tile t belongs to shot s
+// when tile_start[s] <= t < tile_start[s+1]). Warp ty of a block owns a
+// strip of R consecutive rows of the tile: each pressure row of the strip is
+// read once (y neighbours are registers, x neighbours adjacent lanes), and
+// the per-tile work (shot lookup, descriptor, source/receiver list bounds) is
+// shared by R nodes per thread.
+template <typename T>
+struct ShotDesc {
+  T* buf[3];               // rotated like the single-shot fields
+  const T* fact;           // the model's fact (pitched)
+  int64_t px;
+  int32_t nx, ny, halo, gx;  // gx: x tiles of the shot
+  T inv_d[2], inv_d2[2];
+  T* psi[2][2][2];         // [axis][side][parity]
+  BandSide<T> band[2][2];  // coefficients and ξ (ψ pointers filled per step)
+  int32_t active[2][2];
+  int32_t first_r[2];
+  Io<T> io;                // per-tile lists of this shot; rim served by tile 0
+};
+
+template <typename T, int TY, int R>
+__global__ void __launch_bounds__(32 * TY) step2d_batch(const ShotDesc<T>* __restrict__ shots,
+                                                        const int32_t* __restrict__ tile_start,
+                                                        int32_t nshots, int32_t ntiles,
+                                                        int32_t it) {
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  int s = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    // tiles of a block increase, so the shot index only moves forward
+    while (s + 1 < nshots && __ldg(tile_start + s + 1) <= t) ++s;
+    const ShotDesc<T>& D = shots[s];
+    const int local = t - __ldg(tile_start + s);
+    const int nx = D.nx, ny = D.ny, halo = D.halo;
+    T* pnew = D.buf[(it + 2) % 3];
+    if (local == 0 && D.io.nrim > 0) {
+      Io<T> io = D.io;
+      rim_io(io, pnew, it);
+    }
+    const int x0 = (local % D.gx) * 32;
+    const int i = x0 + tx;
+    const int j0 = 1 + (local / D.gx) * (TY * R) + ty * R;
+    if (j0 > ny - 2) continue;  // whole warp
+    const int64_t px = D.px;
+    const T* __restrict__ pcur = D.buf[(it + 1) % 3];
+    const T* __restrict__ pold = D.buf[it % 3];
+    const int e0 = D.io.blk_off[local], e1 = D.io.blk_off[local + 1];
+    // Load phase, free of branches so that all loads of the strip are in
+    // flight together: R + 2 pressure rows, R rows of the old field and of
+    // fact. Rows past the grid are clamped to the last rows (their values are
+    // never stored); x neighbours come from the adjacent lanes, and lanes 0
+    // and 31 also load the node just outside the 32-node strip (clamped into
+    // [0, nx-1]; a clamped value is never used).
+    T pcv[R + 2], pov[R], fv[R], xe[R];
+    const int ie = tx == 0 ? max(x0 - 1, 0) : min(x0 + 32, nx - 1);
+    const bool edge = tx == 0 || tx == 31;
+#pragma unroll
+    for (int r = 0; r < R + 2; ++r) pcv[r] = __ldg(pcur + i + px * min(j0 - 1 + r, ny - 1));
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int64_t row = px * min(j0 + r, ny - 2);
+      pov[r] = __ldg(pold + i + row);
+      fv[r] = __ldg(D.fact + i + row);
+      xe[r] = edge ? __ldg(pcur + ie + row) : T(0);
+    }
+    const bool live = i >= 1 && i <= nx - 2;
+    // Fast path: the warp's 32 x R strip meets no active CPML band and holds
+    // no source or receiver.
+    const bool xband = (D.active[0][0] && x0 <= halo) ||
+                       (D.active[0][1] && x0 + 31 >= nx - halo - 1);
+    const bool yband = (D.active[1][0] && j0 <= halo) ||
+                       (D.active[1][1] && j0 + R - 1 >= ny - halo - 1);
+    if (!xband && !yband && e0 == e1) {
+      const T cx = D.inv_d2[0], cy = D.inv_d2[1];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const T pc = pcv[r + 1];
+        T xm = __shfl_up_sync(0xffffffffu, pc, 1), xp = __shfl_down_sync(0xffffffffu, pc, 1);
+        if (tx == 0) xm = xe[r];
+        if (tx == 31) xp = xe[r];
+        const T d2x = second_diff(xm, pc, xp, cx);
+        const T d2y = second_diff(pcv[r], pc, pcv[r + 2], cy);
+        if (live && j0 + r <= ny - 2) pnew[i + px * (j0 + r)] = leapfrog2d(pc, pov[r], fv[r], d2x, d2y);
+      }
+      continue;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = j0 + r;
+      const T ym = pcv[r], pc = pcv[r + 1], yp = pcv[r + 2];
+      T xm = __shfl_up_sync(0xffffffffu, pc, 1), xp = __shfl_down_sync(0xffffffffu, pc, 1);
+      if (tx == 0) xm = xe[r];
+      if (tx == 31) xp = xe[r];
+      if (!live || j > ny - 2) continue;
+      const int64_t o = (int64_t)i + px * j;
+      const T po = pov[r], f = fv[r];
+      const T d2x = second_diff(xm, pc, xp, D.inv_d2[0]);
+      const T d2y = second_diff(ym, pc, yp, D.inv_d2[1]);
+      T v = leapfrog2d(pc, po, f, d2x, d2y);
+      int q;
+      bool first;
+      const int bx = band_of(i, nx, halo, D.first_r[0], q, first);
+      const int by = band_of(j, ny, halo, D.first_r[1], q, first);
+      if ((bx != 0 && D.active[0][bx - 1]) || (by != 0 && D.active[1][by - 1])) {
+        T damp = 0;
+        if (bx != 0 && D.active[0][bx - 1]) {
+          BandSide<T> B = D.band[0][bx - 1];
+          B.psi_old = D.psi[0][bx - 1][it & 1];
+          B.psi_new = D.psi[0][bx - 1][(it + 1) & 1];
+          band_of(i, nx, halo, D.first_r[0], q, first);
+          band_axis(B, q, first, xm, pc, xp, d2x, f, D.inv_d[0], (int64_t)(halo + 1) * j,
+                    (int64_t)halo * j, (int64_t)1, damp);
+        }
+        if (by != 0 && D.active[1][by - 1]) {
+          BandSide<T> B = D.band[1][by - 1];
+          B.psi_old = D.psi[1][by - 1][it & 1];
+          B.psi_new = D.psi[1][by - 1][(it + 1) & 1];
+          band_of(j, ny, halo, D.first_r[1], q, first);
+          band_axis(B, q, first, ym, pc, yp, d2y, f, D.inv_d[1], (int64_t)i, (int64_t)i, px,
+                    damp);
+        }
+        v += damp;
+      }
+      const int lidx = tx + 32 * (ty * R + r);
+      for (int e = e0; e < e1; ++e) {
+        const int4 en = D.io.ent[e];
+        if (en.x == lidx) v = node_io(D.io, it, en.z, en.w, v);
+      }
+      pnew[o] = v;
+    }
+  }
 }
 
 // fact = (dt^2) * (vel^2) in FP64, rounded once to T (acoustic_3D_xPU.jl:242);

@@ -70,6 +70,61 @@ def config2(nt=2000, seed=1234, interior=256):
                 kwargs=dict(halo=halo, rcoef=1e-4, freetop=True, dt=dt, nt=nt))
 
 
+CONFIG3_INTERIORS = ((512, 256), (768, 384), (1024, 512), (1536, 768), (2048, 1024),
+                     (1024, 1024))
+
+
+def layered_model(rng, nx, ny, halo, dx):
+    """Layered velocity 1500-4500 m/s with 3-8 interfaces at seeded depths,
+    increasing downwards with seeded jumps, times (1 + 3% seeded
+    Gaussian-smoothed noise, sigma = 4 nodes)."""
+    nint = int(rng.integers(3, 9))
+    depths = np.sort(rng.choice(np.arange(8, ny - 8), size=nint, replace=False))
+    v = np.sort(rng.uniform(1500.0, 4500.0, size=nint + 1))
+    v[0], v[-1] = 1500.0, 4500.0
+    col = np.full(ny, v[0])
+    for k, j in enumerate(depths):
+        col[j:] = v[k + 1]
+    noise = gaussian_smooth(rng.standard_normal((nx, ny)), 4.0)
+    noise *= 0.03 / np.abs(noise).max()
+    return np.asfortranarray(col[None, :] * (1.0 + noise))
+
+
+def config3(nt=3000, seed=4321, shots_per_model=16, interiors=CONFIG3_INTERIORS, halo=20,
+            dx=5.0):
+    """2D batched shots: one layered model per interior size (nx x ny interior,
+    512 x 256, 768 x 384, 1024 x 512, 1536 x 768, 2048 x 1024, 1024 x 1024;
+    grid interior + 2 halo by interior + halo with a free top), dx = dy = 5 m, halo 20, R = 1e-4, each model's own CFL step
+    dt = sqrt(2) / (cmax (1/dx + 1/dy)) / 2, nt common. Each model carries
+    `shots_per_model` Ricker shots evenly spaced along depth node j = 3 with
+    f0 ~ U(10, 20) Hz and t0 = 1.2 / f0, and receivers on every 4th node of
+    j = 3 inside the interior."""
+    rng = np.random.default_rng(seed)
+    models, shots = [], []
+    for m, (ix, iy) in enumerate(interiors):
+        nx, ny = ix + 2 * halo, iy + halo
+        vel = layered_model(rng, nx, ny, halo, dx)
+        models.append(((nx - 1) * dx, (ny - 1) * dx, vel))
+        rec = [[(i - 1) * dx, 2 * dx] for i in range(halo + 1, nx - halo + 1, 4)]
+        for s in range(shots_per_model):
+            i = halo + 1 + round((s + 0.5) * (ix - 1) / shots_per_model)
+            f0 = float(rng.uniform(10.0, 20.0))
+            shots.append(dict(model=m, src_pos=[[(i - 1) * dx, 2 * dx]], t0s=[1.2 / f0],
+                              f0=f0, rec_pos=rec))
+    return dict(name=f"cpml2d_batch_{len(models)}models_{len(shots)}shots_nt{nt}",
+                models=models, shots=shots,
+                kwargs=dict(halo=halo, rcoef=1e-4, freetop=True, nt=nt))
+
+
+def batch_shots(pkg, w):
+    """(model index, Sources, Receivers) per shot of a batched workload."""
+    out = []
+    for sh in w["shots"]:
+        srcs = pkg.Sources(sh["src_pos"], sh["t0s"], [pkg.rickersource1D], sh["f0"])
+        out.append((sh["model"], srcs, pkg.Receivers(sh["rec_pos"])))
+    return out
+
+
 def sources_receivers(pkg, w):
     """Sources/Receivers objects (Ricker source functions) of a workload."""
     srcs = pkg.Sources(w["src_pos"], w["t0s"], [pkg.rickersource1D] * len(w["t0s"]), w["f0"])

@@ -159,6 +159,51 @@ int awc_plan_get_launch(const awc_plan* plan, int32_t* tile_y, int32_t* zchunk,
  * step [ms] to best_ms_per_step when not NULL. */
 int awc_plan_autotune(awc_plan* plan, int64_t steps, float* best_ms_per_step);
 
+/* ---- Batched 2D shots ----------------------------------------------------
+ * Many shots over several 2D velocity models of uneven size advance together:
+ * one kernel launch per time step covers every shot, and the nt-step loop is
+ * one CUDA graph. Each shot computes what awc_forward computes for the same
+ * problem. No counterpart in the reference, whose solve2D runs one shot per
+ * call (src/shared/acoustic_2D_xPU.jl:133-445). */
+typedef struct awc_shot {
+  int32_t model;          /* index of the shot's velocity model */
+  int32_t nsrc, nrec;
+  const double* coeffs;   /* packed CPML coefficients of the shot (they depend
+                             on its f0 through alpha_max = pi f0) */
+  const int64_t* possrcs; /* (nsrc x 2) 1-based nodes */
+  const double* dt2srctf; /* (nt x nsrc) scaled source time functions */
+  const int64_t* posrecs; /* (nrec x 2) 1-based nodes */
+} awc_shot;
+
+typedef struct awc_batch awc_batch;
+
+/* models[m]: model m (ndim = 2; every model has the same precision and nt;
+ * its own nx, ny, dx, dy, dt, halo; nsrc/nrec ignored); vel[m]: its velocity
+ * (nx*ny, column-major). */
+int awc_batch_create(awc_ctx* ctx, int32_t nmodels, const awc_problem* models,
+                     const double* const* vel, int32_t nshots, const awc_shot* shots,
+                     awc_batch** out);
+void awc_batch_destroy(awc_batch* batch);
+int awc_batch_reset(awc_batch* batch);
+/* Same contract as awc_plan_run, for every shot of the batch. */
+int awc_batch_run(awc_batch* batch, int64_t nsteps, int32_t use_graph, float* ms);
+int64_t awc_batch_step(const awc_batch* batch);
+/* One shot's traces (nt x nrec) and current field (nx*ny), as doubles. */
+int awc_batch_traces(awc_batch* batch, int32_t shot, double* traces);
+int awc_batch_field(awc_batch* batch, int32_t shot, double* p);
+/* Tile height (4, 8, 16, 32 or 64 rows of 32 nodes; 4 warps per block, each
+ * streaming tile_y/4 rows) and resident blocks per SM (1..32) of the
+ * persistent step kernel; results do not depend on them. */
+int awc_batch_set_launch(awc_batch* batch, int32_t tile_y, int32_t blocks_per_sm);
+int awc_batch_get_launch(const awc_batch* batch, int32_t* tile_y, int32_t* blocks_per_sm);
+/* Times every launch shape on the batch's data, keeps the fastest, resets. */
+int awc_batch_autotune(awc_batch* batch, int64_t steps, float* best_ms_per_step);
+/* create + autotune (nt >= 100) + run(nt) + every shot's traces + destroy;
+ * traces[s] is shot s's (nt x nrec) output. */
+int awc_forward_batch(awc_ctx* ctx, int32_t nmodels, const awc_problem* models,
+                      const double* const* vel, int32_t nshots, const awc_shot* shots,
+                      double* const* traces);
+
 /* awc_forward for 2D FP32 problems without any device memory allocation.
  * No counterpart in the reference (its solvers always allocate).
  *
