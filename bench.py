@@ -219,6 +219,47 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def batch_leg(pkg, ctx, args, rank, world, timed, peak):
+    """Batched 2D shots, FP32: the 96 shots of the six-model layered workload,
+    rank r taking shots r, r + N, ... (no data-path collective). One step of
+    this leg = every shot of the rank's batch advanced over all nt time steps
+    (one CUDA graph replay); time = max over ranks."""
+    from acousticwavecpml_b200 import workloads as W
+    w = W.config3()
+    shots = W.batch_shots(pkg, w)
+    mine = shots[rank::world]
+    probs, vels, setups, idx = pkg.prepare_batch(w["models"], mine, **w["kwargs"])
+    b = pkg.Batch(ctx, probs, vels, setups, idx)
+    b.autotune(20)
+    nt = b.nt
+
+    def run():
+        b.reset()
+        b.run(nt, graph=True)
+
+    run()
+    k = 2
+    ms = timed(run, k)
+    words = sum(pkg.core.a_eff_words(st["problem"]) for st in setups)
+    nodes = sum(st["problem"].nx * st["problem"].ny for st in setups)
+    t_ts = ms / 1e3 / (k * nt)
+    ty, bps = b.get_launch()
+    b.close()
+    achieved = words * 4 / t_ts / 1e9
+    return {"workload": w["name"], "shots": len(shots), "models": len(w["models"]),
+            "nt": nt, "dtype": "f32", "value": len(shots) / (ms / 1e3 / k), "unit": "shots/s",
+            "us_per_timestep": t_ts * 1e6, "gnodes_per_s": world * nodes / t_ts / 1e9,
+            "t_eff_gbs": world * achieved,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "per_launch": "one time step of every shot of the rank's batch = one "
+                                       "persistent step2d_batch launch; A_eff summed over "
+                                       "shots, FP32 words"},
+            "launch": {"tile": [32, ty], "blocks_per_sm": bps},
+            "gpu_launches": k * nt, "timed_runs": k,
+            "sharding": f"shots {rank}::{world} per rank" if world > 1 else "one batch"}
+
+
 def main():
     args = parse_args()
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -367,6 +408,9 @@ def main():
             nrm = np.linalg.norm(tr64)
             line["fp32_vs_fp64_traces_rel_l2"] = float(np.linalg.norm(traces_dev - tr64) /
                                                        (nrm if nrm > 0 else 1.0))
+
+        # ---- batched 2D shots (96 shots over 6 layered models), sharded -----
+        line["batch"] = batch_leg(pkg, ctx, args, rank, world, timed, peak)
 
         # ---- CPU baseline (rank 0 at N=1 only) ------------------------------
         if world == 1 and rank == 0:
