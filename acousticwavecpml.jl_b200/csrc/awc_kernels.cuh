@@ -111,11 +111,12 @@ struct StepParams {
   int32_t shell_zchunk;  // planes per block of the band kernel
 };
 
-// The 2D node update with its rounding pinned, so that every 2D kernel (one
-// shot, batched shots, either path of the batched kernel) gives bitwise the
-// same value: each second difference is rounded on its own (a multiply the
-// compiler may not fuse into the following add), then the leapfrog is one
-// fused multiply-add, 2 pc - po + f (d2x + d2y).
+// Node arithmetic with its rounding pinned. Every kernel forms a second
+// difference with a multiply the compiler may not fuse into the following
+// add, the leapfrog as one fused multiply-add 2 pc - po + f (Σ d2), and the
+// CPML recursions with explicit fused multiply-adds. So the result of a node
+// does not depend on which copy of the code computes it: batched and
+// single-shot 2D kernels agree bitwise, and so do all launch shapes.
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 template <typename T>
@@ -125,6 +126,37 @@ __device__ __forceinline__ T second_diff(T m, T c, T p, T inv_d2) {
 template <typename T>
 __device__ __forceinline__ T leapfrog2d(T pc, T po, T f, T d2x, T d2y) {
   return fma(f, d2x + d2y, T(2) * pc - po);
+}
+template <typename T>
+__device__ __forceinline__ T leapfrog3d(T pc, T po, T f, T d2x, T d2y, T d2z) {
+  return fma(f, d2x + d2y + d2z, T(2) * pc - po);
+}
+
+// The CPML coefficients of one band entry q: half-grid b/K and a at q and
+// q-1, on-grid b/K and a at q-1.
+template <typename T>
+struct BandCoef {
+  T bh, ah, bhm, ahm, bk, a;
+};
+template <typename T>
+__device__ __forceinline__ BandCoef<T> band_coef(const BandSide<T>& B, int q) {
+  return BandCoef<T>{__ldg(B.bKh + q), __ldg(B.ah + q), __ldg(B.bKh + q - 1),
+                     __ldg(B.ah + q - 1), __ldg(B.bK + q - 1), __ldg(B.a + q - 1)};
+}
+// One axis of the CPML band update at one node (update_ψ! on both faces of
+// the node, then the ξ recursion and the damping term of update_p!):
+// ψ[q] = b/K_half[q] ψ[q] + a_half[q] (pp - pc) / d, ψ[q-1] likewise with
+// (pc - pm); dψ = (ψ[q] - ψ[q-1]) / d; ξ = b/K[q-1] ξ + a[q-1] (d2 + dψ);
+// damp += f (dψ + ξ).
+template <typename T>
+__device__ __forceinline__ void cpml_axis(const BandCoef<T>& c, T psq, T psm, T xo, T pm, T pc,
+                                          T pp, T d2, T f, T inv, T& sq, T& sm, T& xn,
+                                          T& damp) {
+  sq = fma(c.bh, psq, mul_rn(mul_rn(c.ah, pp - pc), inv));
+  sm = fma(c.bhm, psm, mul_rn(mul_rn(c.ahm, pc - pm), inv));
+  const T dps = mul_rn(sq - sm, inv);
+  xn = fma(c.bk, xo, mul_rn(c.a, d2 + dps));
+  damp = fma(f, dps + xn, damp);
 }
 
 // Which band (if any) coordinate c of an axis of length n lies in.
@@ -154,15 +186,12 @@ __device__ __forceinline__ void band_axis(const BandSide<T>& B, int q, bool firs
                                           int64_t xi_base, int64_t stride, T& damp) {
   const T ps_q_old = B.psi_old[psi_base + (int64_t)q * stride];
   const T ps_m_old = B.psi_old[psi_base + (int64_t)(q - 1) * stride];
-  const T ps_q = B.bKh[q] * ps_q_old + B.ah[q] * (pp - pc) * inv_d;
-  const T ps_m = B.bKh[q - 1] * ps_m_old + B.ah[q - 1] * (pc - pm) * inv_d;
-  B.psi_new[psi_base + (int64_t)q * stride] = ps_q;
-  if (first) B.psi_new[psi_base + (int64_t)(q - 1) * stride] = ps_m;
-  const T dpsi = (ps_q - ps_m) * inv_d;
   T* xp = B.xi + xi_base + (int64_t)(q - 1) * stride;
-  const T xn = B.bK[q - 1] * (*xp) + B.a[q - 1] * (d2 + dpsi);
+  T sq, sm, xn;
+  cpml_axis(band_coef(B, q), ps_q_old, ps_m_old, *xp, pm, pc, pp, d2, f, inv_d, sq, sm, xn, damp);
+  B.psi_new[psi_base + (int64_t)q * stride] = sq;
+  if (first) B.psi_new[psi_base + (int64_t)(q - 1) * stride] = sm;
   *xp = xn;
-  damp += f * (dpsi + xn);
 }
 
 // Sources then receivers of one node, for the thread that owns its value v.
@@ -269,33 +298,6 @@ struct Tile3 {
   static constexpr int BYTES = PC_PAD + 2 * IN_BYTES;
 };
 
-// CPML band work of one node: every active band axis the node lies in.
-template <typename T>
-__device__ __forceinline__ T band_node(const StepParams<T>& P, int i, int j, int k, T pc, T xm,
-                                       T xp, T ym, T yp, T pm, T pp, T d2x, T d2y, T d2z, T f) {
-  T damp = 0;
-  int q;
-  bool first;
-  const int bx = band_of(i, P.nx, P.halo, P.first_r[0], q, first);
-  if (bx != 0 && P.active[0][bx - 1]) {
-    const int64_t jk = (int64_t)j + (int64_t)P.ny * k;
-    band_axis(P.band[0][bx - 1], q, first, xm, pc, xp, d2x, f, P.inv_d[0],
-              (int64_t)(P.halo + 1) * jk, (int64_t)P.halo * jk, (int64_t)1, damp);
-  }
-  const int by = band_of(j, P.ny, P.halo, P.first_r[1], q, first);
-  if (by != 0 && P.active[1][by - 1]) {
-    band_axis(P.band[1][by - 1], q, first, ym, pc, yp, d2y, f, P.inv_d[1],
-              (int64_t)i + P.px * (P.halo + 1) * k, (int64_t)i + P.px * P.halo * k, P.px, damp);
-  }
-  const int bz = band_of(k, P.nz, P.halo, P.first_r[2], q, first);
-  if (bz != 0 && P.active[2][bz - 1]) {
-    const int64_t c = (int64_t)i + P.px * j;
-    band_axis(P.band[2][bz - 1], q, first, pm, pc, pp, d2z, f, P.inv_d[2], c, c, P.px * P.ny,
-              damp);
-  }
-  return damp;
-}
-
 // ---------------------------------------------------------------------------
 // 3D core step: the nodes of P.core, which lie outside every active CPML
 // band, so no band state is touched. Grid: x tiles of 64 nodes from P.core_x,
@@ -393,18 +395,14 @@ __global__ void __launch_bounds__(32 * TY) step3d_core(const __grid_constant__ C
     const V2 f_0 = *reinterpret_cast<const V2*>(ff + i0);
     const V2 f_1 = *reinterpret_cast<const V2*>(ff + i0 + L::TX);
     // node (row, x): 2 pcur - pold + fact * (d2x + d2y + d2z)
-    T v00 = T(2) * c_0.x - po0.x +
-            f_0.x * ((c_0.y - T(2) * c_0.x + xm0) * ix2 + (c_1.x - T(2) * c_0.x + ym.x) * iy2 +
-                     (zp0.x - T(2) * c_0.x + zm0.x) * iz2);
-    T v01 = T(2) * c_0.y - po0.y +
-            f_0.y * ((xp0 - T(2) * c_0.y + c_0.x) * ix2 + (c_1.y - T(2) * c_0.y + ym.y) * iy2 +
-                     (zp0.y - T(2) * c_0.y + zm0.y) * iz2);
-    T v10 = T(2) * c_1.x - po1.x +
-            f_1.x * ((c_1.y - T(2) * c_1.x + xm1) * ix2 + (yp.x - T(2) * c_1.x + c_0.x) * iy2 +
-                     (zp1.x - T(2) * c_1.x + zm1.x) * iz2);
-    T v11 = T(2) * c_1.y - po1.y +
-            f_1.y * ((xp1 - T(2) * c_1.y + c_1.x) * ix2 + (yp.y - T(2) * c_1.y + c_0.y) * iy2 +
-                     (zp1.y - T(2) * c_1.y + zm1.y) * iz2);
+    T v00 = leapfrog3d(c_0.x, po0.x, f_0.x, second_diff(xm0, c_0.x, c_0.y, ix2),
+                       second_diff(ym.x, c_0.x, c_1.x, iy2), second_diff(zm0.x, c_0.x, zp0.x, iz2));
+    T v01 = leapfrog3d(c_0.y, po0.y, f_0.y, second_diff(c_0.x, c_0.y, xp0, ix2),
+                       second_diff(ym.y, c_0.y, c_1.y, iy2), second_diff(zm0.y, c_0.y, zp0.y, iz2));
+    T v10 = leapfrog3d(c_1.x, po1.x, f_1.x, second_diff(xm1, c_1.x, c_1.y, ix2),
+                       second_diff(c_0.x, c_1.x, yp.x, iy2), second_diff(zm1.x, c_1.x, zp1.x, iz2));
+    T v11 = leapfrog3d(c_1.y, po1.y, f_1.y, second_diff(c_1.x, c_1.y, xp1, ix2),
+                       second_diff(c_0.y, c_1.y, yp.y, iy2), second_diff(zm1.y, c_1.y, zp1.y, iz2));
     // sources and receivers of this plane (block-uniform walk, rarely taken)
     for (; ioe < ioe1; ++ioe) {
       const int4 en = P.io.ent[ioe];
@@ -459,14 +457,11 @@ template <typename T>
 __device__ __forceinline__ void band_apply(const BandSide<T>& B, int q, bool first, int64_t pq,
                                            int64_t dq, int64_t xq, T psq, T psm, T xo, T pm,
                                            T pc, T pp, T d2, T f, T inv, T& damp) {
-  const T sq = __ldg(B.bKh + q) * psq + __ldg(B.ah + q) * (pp - pc) * inv;
-  const T sm = __ldg(B.bKh + q - 1) * psm + __ldg(B.ah + q - 1) * (pc - pm) * inv;
+  T sq, sm, xn;
+  cpml_axis(band_coef(B, q), psq, psm, xo, pm, pc, pp, d2, f, inv, sq, sm, xn, damp);
   B.psi_new[pq] = sq;
   if (first) B.psi_new[pq - dq] = sm;
-  const T dps = (sq - sm) * inv;
-  const T xn = __ldg(B.bK + q - 1) * xo + __ldg(B.a + q - 1) * (d2 + dps);
   B.xi[xq] = xn;
-  damp += f * (dps + xn);
 }
 
 // ---------------------------------------------------------------------------
@@ -556,10 +551,10 @@ __global__ void __launch_bounds__(256) step3d_band(StepParams<T> P) {
       }
       const T xm = __ldg(pcur + o - 1), xp = __ldg(pcur + o + 1);
       const T ym = __ldg(pcur + o - px), yp = __ldg(pcur + o + px);
-      const T d2x = (xp - T(2) * pc + xm) * P.inv_d2[0];
-      const T d2y = (yp - T(2) * pc + ym) * P.inv_d2[1];
-      const T d2z = (pp - T(2) * pc + pm) * P.inv_d2[2];
-      v = T(2) * pc - po + f * (d2x + d2y + d2z);
+      const T d2x = second_diff(xm, pc, xp, P.inv_d2[0]);
+      const T d2y = second_diff(ym, pc, yp, P.inv_d2[1]);
+      const T d2z = second_diff(pm, pc, pp, P.inv_d2[2]);
+      v = leapfrog3d(pc, po, f, d2x, d2y, d2z);
       T damp = 0;
       if (sx)
         band_apply(P.band[0][sx - 1], qx, fx, pqx, (int64_t)1, xqx, xq, xmq, xx, xm, pc, xp, d2x,

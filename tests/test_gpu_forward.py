@@ -111,6 +111,17 @@ CASES3D = {
     "odd_sizes": lambda: small3d(n=(37, 45, 19), halo=4, freetop=True),
     "thin_z": lambda: small3d(n=(70, 40, 5), halo=1, freetop=False,
                               srcs=[[300.0, 200.0, 20.0]], recs=[[100.0, 100.0, 20.0]]),
+    # a core box with all three band launches around it (x band tiles, y band
+    # rows, z band planes), sources and receivers in each part
+    "core_and_bands": lambda: small3d(
+        n=(100, 90, 80), halo=20, freetop=False, lt=0.12,
+        srcs=[[490.0, 400.0, 390.0], [100.0, 450.0, 300.0], [500.0, 820.0, 100.0]],
+        recs=[[(i - 1) * 10.0, (j - 1) * 10.0, (k - 1) * 10.0]
+              for i, j, k in ((5, 5, 5), (30, 40, 40), (60, 85, 40), (97, 45, 78), (50, 45, 10),
+                              (33, 40, 40), (64, 70, 21), (65, 70, 60), (2, 2, 2))]),
+    # a halo wider than one 32-node x tile, free top
+    "wide_halo_freetop": lambda: small3d(n=(133, 70, 90), halo=34, freetop=True, lt=0.1,
+                                         srcs=[[660.0, 300.0, 450.0], [100.0, 30.0, 50.0]]),
 }
 
 
