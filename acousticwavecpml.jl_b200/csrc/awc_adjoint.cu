@@ -1,0 +1,584 @@
+// Discrete adjoint of the CPML time step, with checkpointing, for the
+// gradient of a least-squares trace misfit with respect to c² and for the
+// transpose of the source-to-trace map.
+//
+// The forward step t (0-based, awc_kernels.cuh) maps the state
+// (p_{t-1}, p_t, ψ_t, ξ_t) to (p_t, p_{t+1}, ψ_{t+1}, ξ_{t+1}); per axis and
+// CPML side, with faces e = 0..h between nodes c_e and c_e + 1 and band nodes
+// c with entry q = 1..h (c = q + off, off = 0 on the left, n - h - 2 on the
+// right):
+//   ψ_{t+1}[e]  = bKh_e ψ_t[e] + ah_e (p_t[c_e + 1] - p_t[c_e]) / d
+//   ξ_{t+1}[q-1] = bK_{q-1} ξ_t[q-1] + a_{q-1} (D2 p_t(c) + (ψ_{t+1}[q] - ψ_{t+1}[q-1]) / d)
+//   p_{t+1}(c)  = 2 p_t(c) - p_{t-1}(c)
+//                 + F(c) (Σ_axes D2 p_t(c) + Σ_bands ((ψ_{t+1}[q] - ψ_{t+1}[q-1]) / d + ξ_{t+1}[q-1]))
+//                 + S_t(c),                  traces_t[r] = p_{t+1}(c_r),
+// with F = dt² c². For fixed F this is linear in the state. Its exact
+// transpose, run backwards in time with adjoint fields λ (of p), μ (of ψ) and
+// ν (of ξ), is, for interior nodes c:
+//   λ_{t+1}(c) = R_t(c) + 2 λ_{t+2}(c) - λ_{t+3}(c)
+//                + Σ_axes D2ᵀ[F λ_{t+2} + a ν_{t+2}](c)
+//                + Σ_bands (ah_{e1} μ_{t+2}[e1] - ah_{e2} μ_{t+2}[e2]) / d
+//     (e1, e2: the faces left and right of c; R_t: the trace residuals of
+//     step t at the receiver nodes),
+//   ν_{t+1}[q-1] = bK_{q-1} ν_{t+2}[q-1] + F(c) λ_{t+1}(c),
+//   μ_{t+1}[e]   = bKh_e μ_{t+2}[e] + (w_e - w_{e+1}) / d,
+//     w_q = a_{q-1} ν_{t+1}[q-1] + F(c_q) λ_{t+1}(c_q) (0 outside q = 1..h),
+// and dJ/dF(c) = Σ_t λ_{t+1}(c) B_t(c), where B_t is the bracket multiplying
+// F, B_t = (p_{t+1} - 2 p_t + p_{t-1} - S_t)(c) / F(c). Rim nodes carry no
+// adjoint: their values never depend on the interior or on c². Sides whose
+// recursion is trivial (the free top) feed nothing back and are skipped, as
+// in the forward. Bands must not overlap (n >= 2 halo + 2 on every axis with
+// an active side).
+//
+// Checkpointing: the forward run saves the full state every k steps; the
+// backward pass, segment by segment from the last, restores a checkpoint,
+// recomputes the segment's pressure fields and runs the adjoint steps of the
+// segment in reverse.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/awcpml.h"
+#include "awc_ctx.h"
+#include "awc_kernels.cuh"
+
+namespace awc {
+
+template <typename T>
+struct AdjParams {
+  int32_t ndim, nx, ny, nz, halo;
+  int64_t px, plane;
+  T inv_d[3], inv_d2[3];
+  const T* F;
+  const T* lam2;  // λ_{t+2}
+  const T* lam3;  // λ_{t+3}
+  T* lamn;        // λ_{t+1}
+  T* mu[3][2];    // μ, updated in place (layout of ψ)
+  const T* nu_old[3][2];  // ν_{t+2} (layout of ξ)
+  T* nu_new[3][2];        // ν_{t+1}
+  const T* a[3][2];
+  const T* bK[3][2];
+  const T* ah[3][2];
+  const T* bKh[3][2];
+  int32_t active[3][2];
+  int32_t off[3][2];  // band node c has entry q = c - off
+};
+
+// Element index of entry e of a band array (ψ: h+1 layers, ξ: h layers) of
+// axis a at the node (i, j, k) (the node's own axis coordinate is replaced
+// by e): x (layers, ny, nz); y (px, layers, nz); z (px, ny, layers).
+template <typename T>
+__device__ __forceinline__ int64_t band_index(const AdjParams<T>& A, int a, int layers, int e,
+                                              int i, int j, int k) {
+  if (a == 0) return e + (int64_t)layers * (j + (int64_t)A.ny * k);
+  if (a == 1) return i + A.px * (e + (int64_t)layers * k);
+  return i + A.px * (j + (int64_t)A.ny * e);
+}
+
+template <typename T>
+__device__ __forceinline__ bool interior(const AdjParams<T>& A, int i, int j, int k) {
+  return i >= 1 && i <= A.nx - 2 && j >= 1 && j <= A.ny - 2 &&
+         (A.ndim == 2 || (k >= 1 && k <= A.nz - 2));
+}
+
+// F λ_{t+2} + a ν_{t+2} of axis a at node (i, j, k), 0 off the interior.
+template <typename T>
+__device__ __forceinline__ T adj_g(const AdjParams<T>& A, int a, int i, int j, int k) {
+  if (!interior(A, i, j, k)) return T(0);
+  const int64_t o = i + A.px * j + A.plane * k;
+  T g = A.F[o] * A.lam2[o];
+  const int c = a == 0 ? i : a == 1 ? j : k;
+  for (int s = 0; s < 2; ++s) {
+    if (!A.active[a][s]) continue;
+    const int q = c - A.off[a][s];
+    if (q >= 1 && q <= A.halo)
+      g += A.a[a][s][q - 1] * A.nu_old[a][s][band_index(A, a, A.halo, q - 1, i, j, k)];
+  }
+  return g;
+}
+
+// λ_{t+1} without the receiver residuals.
+template <typename T>
+__global__ void __launch_bounds__(256) adj_lambda(AdjParams<T> A) {
+  const int i = 1 + blockIdx.x * 32 + threadIdx.x;
+  const int j = 1 + blockIdx.y * 8 + threadIdx.y;
+  const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
+  if (i > A.nx - 2 || j > A.ny - 2) return;
+  const int64_t o = i + A.px * j + A.plane * k;
+  T lam = T(2) * A.lam2[o] - A.lam3[o];
+  for (int a = 0; a < A.ndim; ++a) {
+    const int di = a == 0, dj = a == 1, dk = a == 2;
+    const T gm = adj_g(A, a, i - di, j - dj, k - dk);
+    const T g0 = adj_g(A, a, i, j, k);
+    const T gp = adj_g(A, a, i + di, j + dj, k + dk);
+    lam += A.inv_d2[a] * (gp - T(2) * g0 + gm);
+    const int c = a == 0 ? i : a == 1 ? j : k;
+    for (int s = 0; s < 2; ++s) {
+      if (!A.active[a][s]) continue;
+      const int e1 = c - 1 - A.off[a][s], e2 = c - A.off[a][s];
+      if (e1 >= 0 && e1 <= A.halo)
+        lam += A.inv_d[a] * A.ah[a][s][e1] *
+               A.mu[a][s][band_index(A, a, A.halo + 1, e1, i, j, k)];
+      if (e2 >= 0 && e2 <= A.halo)
+        lam -= A.inv_d[a] * A.ah[a][s][e2] *
+               A.mu[a][s][band_index(A, a, A.halo + 1, e2, i, j, k)];
+    }
+  }
+  A.lamn[o] = lam;
+}
+
+// λ_{t+1} += the residuals of step t at the receiver nodes (one thread per
+// node, its receivers summed in receiver order).
+template <typename T>
+__global__ void adj_residuals(T* __restrict__ lamn, const int64_t* __restrict__ node,
+                              const int32_t* __restrict__ off, const int32_t* __restrict__ ids,
+                              int32_t nnode, const T* __restrict__ res_row) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nnode) return;
+  T v = lamn[node[n]];
+  for (int e = off[n]; e < off[n + 1]; ++e) v += res_row[ids[e]];
+  lamn[node[n]] = v;
+}
+
+// ν_{t+1} and the gradient accumulation dJ/dF += λ_{t+1} (p_{t+1} - 2 p_t +
+// p_{t-1}) / F (the source term is removed by adj_sources).
+template <typename T>
+__global__ void __launch_bounds__(256) adj_nu_grad(AdjParams<T> A, const T* __restrict__ pm1,
+                                                   const T* __restrict__ p0,
+                                                   const T* __restrict__ pp1,
+                                                   double* __restrict__ grad) {
+  const int i = 1 + blockIdx.x * 32 + threadIdx.x;
+  const int j = 1 + blockIdx.y * 8 + threadIdx.y;
+  const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
+  if (i > A.nx - 2 || j > A.ny - 2) return;
+  const int64_t o = i + A.px * j + A.plane * k;
+  const T lam = A.lamn[o], f = A.F[o];
+  for (int a = 0; a < A.ndim; ++a) {
+    const int c = a == 0 ? i : a == 1 ? j : k;
+    for (int s = 0; s < 2; ++s) {
+      if (!A.active[a][s]) continue;
+      const int q = c - A.off[a][s];
+      if (q < 1 || q > A.halo) continue;
+      const int64_t x = band_index(A, a, A.halo, q - 1, i, j, k);
+      A.nu_new[a][s][x] = A.bK[a][s][q - 1] * A.nu_old[a][s][x] + f * lam;
+    }
+  }
+  if (grad) {
+    const double b = ((double)pp1[o] - 2.0 * (double)p0[o] + (double)pm1[o]) / (double)f;
+    grad[o] += (double)lam * b;
+  }
+}
+
+// μ_{t+1} in place: band node q updates face q, the first node also face 0.
+template <typename T>
+__global__ void __launch_bounds__(256) adj_mu(AdjParams<T> A) {
+  const int i = 1 + blockIdx.x * 32 + threadIdx.x;
+  const int j = 1 + blockIdx.y * 8 + threadIdx.y;
+  const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
+  if (i > A.nx - 2 || j > A.ny - 2) return;
+  const int64_t o = i + A.px * j + A.plane * k;
+  for (int a = 0; a < A.ndim; ++a) {
+    const int c = a == 0 ? i : a == 1 ? j : k;
+    const int64_t step = a == 0 ? 1 : a == 1 ? A.px : A.plane;
+    const int di = a == 0, dj = a == 1, dk = a == 2;
+    for (int s = 0; s < 2; ++s) {
+      if (!A.active[a][s]) continue;
+      const int q = c - A.off[a][s];
+      if (q < 1 || q > A.halo) continue;
+      const T wq = A.a[a][s][q - 1] * A.nu_new[a][s][band_index(A, a, A.halo, q - 1, i, j, k)] +
+                   A.F[o] * A.lamn[o];
+      T wn = 0;
+      if (q + 1 <= A.halo)
+        wn = A.a[a][s][q] * A.nu_new[a][s][band_index(A, a, A.halo, q, i + di, j + dj, k + dk)] +
+             A.F[o + step] * A.lamn[o + step];
+      const int64_t m = band_index(A, a, A.halo + 1, q, i, j, k);
+      A.mu[a][s][m] = A.bKh[a][s][q] * A.mu[a][s][m] + A.inv_d[a] * (wq - wn);
+      if (q == 1) {
+        const int64_t m0 = band_index(A, a, A.halo + 1, 0, i, j, k);
+        A.mu[a][s][m0] = A.bKh[a][s][0] * A.mu[a][s][m0] - A.inv_d[a] * wq;
+      }
+    }
+  }
+}
+
+// Per source (one thread each, serial over sources for a fixed summation
+// order): the adjoint of the injected value, λ_{t+1} at the source node,
+// and the removal of the source term from the gradient bracket.
+template <typename T>
+__global__ void adj_sources(const T* __restrict__ lamn, const T* __restrict__ F,
+                            const int64_t* __restrict__ node, int32_t nsrc,
+                            const T* __restrict__ stf_row, double* __restrict__ grad,
+                            T* __restrict__ out_row) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int s = 0; s < nsrc; ++s) {
+    const int64_t o = node[s];
+    if (o < 0) continue;  // rim source: no adjoint
+    if (out_row) out_row[s] = lamn[o];
+    if (grad) grad[o] -= (double)lamn[o] * (double)stf_row[s] / (double)F[o];
+  }
+}
+
+__global__ void scale_unpitch(const double* __restrict__ src, double* __restrict__ dst,
+                              int64_t n, int64_t nx, int64_t px, double scale) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = c % nx, r = c / nx;
+    dst[c] = scale * src[i + px * r];
+  }
+}
+
+template <typename T>
+__global__ void to_double(const T* __restrict__ src, double* __restrict__ dst, int64_t n) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x)
+    dst[c] = (double)src[c];
+}
+
+}  // namespace awc
+
+namespace {
+
+#define ADJ_TRY(C, call)                                                          \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      cudaGetLastError();                                                         \
+      return awc::fail((C), AWC_ERR_CUDA, cudaGetErrorString(e_));                \
+    }                                                                             \
+  } while (0)
+
+// Device memory of one adjoint run, freed on scope exit.
+struct DevMem {
+  std::vector<void*> ptrs;
+  ~DevMem() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+  template <typename P>
+  cudaError_t get(P** out, size_t bytes) {
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 16));
+    if (e == cudaSuccess) ptrs.push_back(p);
+    *out = (P*)p;
+    return e;
+  }
+};
+
+// Interior node groups: each unique interior node of `pos` with its ids.
+struct Groups {
+  std::vector<int64_t> node;
+  std::vector<int32_t> off{0}, ids;
+};
+
+Groups group_nodes(const awc_problem* p, int64_t px, const int64_t* pos, int64_t cnt,
+                   std::vector<int64_t>* per_item) {
+  Groups G;
+  std::unordered_map<int64_t, std::vector<int32_t>> m;
+  std::vector<int64_t> order;
+  const int64_t nz = p->ndim == 3 ? p->nz : 1;
+  if (per_item) per_item->assign(cnt, -1);
+  for (int64_t r = 0; r < cnt; ++r) {
+    const int64_t i = pos[r] - 1, j = pos[r + cnt] - 1, k = p->ndim == 3 ? pos[r + 2 * cnt] - 1 : 0;
+    const bool in = i >= 1 && i <= p->nx - 2 && j >= 1 && j <= p->ny - 2 &&
+                    (p->ndim == 2 || (k >= 1 && k <= nz - 2));
+    if (!in) continue;
+    const int64_t node = i + px * (j + p->ny * k);
+    if (per_item) (*per_item)[r] = node;
+    auto f = m.find(node);
+    if (f == m.end()) {
+      order.push_back(node);
+      m[node] = {(int32_t)r};
+    } else {
+      f->second.push_back((int32_t)r);
+    }
+  }
+  for (int64_t node : order) {
+    G.node.push_back(node);
+    for (int32_t r : m[node]) G.ids.push_back(r);
+    G.off.push_back((int32_t)G.ids.size());
+  }
+  return G;
+}
+
+template <typename T>
+int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t* possrcs,
+                 const double* dt2srctf, const int64_t* posrecs, const double* residual,
+                 int64_t kchk, double* grad_out, double* src_out) {
+  const awc::PlanView V = awc::plan_view(plan);
+  cudaStream_t st = V.stream;
+  const int64_t nt = p->nt, nsrc = p->nsrc, nrec = p->nrec, h = p->halo;
+  const int64_t NP = V.NP, fb = NP * (int64_t)sizeof(T);
+  const bool want_grad = grad_out != nullptr;
+  DevMem mem;
+  // adjoint fields
+  T *lam[2], *mu[3][2] = {}, *nu[3][2][2] = {};
+  for (int b = 0; b < 2; ++b) ADJ_TRY(C, mem.get(&lam[b], fb));
+  for (int a = 0; a < p->ndim; ++a)
+    for (int s = 0; s < 2; ++s) {
+      ADJ_TRY(C, mem.get(&mu[a][s], V.psi_len[a] * sizeof(T)));
+      ADJ_TRY(C, cudaMemsetAsync(mu[a][s], 0, std::max<int64_t>(V.psi_len[a], 1) * sizeof(T), st));
+      for (int b = 0; b < 2; ++b) {
+        ADJ_TRY(C, mem.get(&nu[a][s][b], V.xi_len[a] * sizeof(T)));
+        ADJ_TRY(C, cudaMemsetAsync(nu[a][s][b], 0, std::max<int64_t>(V.xi_len[a], 1) * sizeof(T), st));
+      }
+    }
+  for (int b = 0; b < 2; ++b) ADJ_TRY(C, cudaMemsetAsync(lam[b], 0, fb, st));
+  double* grad = nullptr;
+  if (want_grad) {
+    ADJ_TRY(C, mem.get(&grad, NP * sizeof(double)));
+    ADJ_TRY(C, cudaMemsetAsync(grad, 0, NP * sizeof(double), st));
+  }
+  // residual rows [nt][nrec] and source rows [nt][nsrc] in T
+  std::vector<T> rows(std::max<int64_t>(nt * nrec, 1));
+  for (int64_t r = 0; r < nrec; ++r)
+    for (int64_t t = 0; t < nt; ++t) rows[t * nrec + r] = (T)residual[t + nt * r];
+  T* res_d;
+  ADJ_TRY(C, mem.get(&res_d, rows.size() * sizeof(T)));
+  ADJ_TRY(C, cudaMemcpyAsync(res_d, rows.data(), rows.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  std::vector<T> srows(std::max<int64_t>(nt * nsrc, 1), T(0));
+  if (dt2srctf)
+    for (int64_t s = 0; s < nsrc; ++s)
+      for (int64_t t = 0; t < nt; ++t) srows[t * nsrc + s] = (T)dt2srctf[t + nt * s];
+  T* stf_d;
+  ADJ_TRY(C, mem.get(&stf_d, srows.size() * sizeof(T)));
+  ADJ_TRY(C, cudaMemcpyAsync(stf_d, srows.data(), srows.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  T* sout_d = nullptr;
+  if (src_out) ADJ_TRY(C, mem.get(&sout_d, std::max<int64_t>(nt * nsrc, 1) * sizeof(T)));
+  // receiver groups and source nodes (interior only)
+  const Groups RG = group_nodes(p, V.px, posrecs, nrec, nullptr);
+  std::vector<int64_t> snode;
+  group_nodes(p, V.px, possrcs, nsrc, &snode);
+  int64_t* rnode_d;
+  int32_t *roff_d, *rids_d;
+  int64_t* snode_d;
+  ADJ_TRY(C, mem.get(&rnode_d, RG.node.size() * 8));
+  ADJ_TRY(C, mem.get(&roff_d, RG.off.size() * 4));
+  ADJ_TRY(C, mem.get(&rids_d, RG.ids.size() * 4));
+  ADJ_TRY(C, mem.get(&snode_d, snode.size() * 8));
+  if (!RG.node.empty()) {
+    ADJ_TRY(C, cudaMemcpyAsync(rnode_d, RG.node.data(), RG.node.size() * 8, cudaMemcpyHostToDevice, st));
+    ADJ_TRY(C, cudaMemcpyAsync(rids_d, RG.ids.data(), RG.ids.size() * 4, cudaMemcpyHostToDevice, st));
+  }
+  ADJ_TRY(C, cudaMemcpyAsync(roff_d, RG.off.data(), RG.off.size() * 4, cudaMemcpyHostToDevice, st));
+  if (!snode.empty())
+    ADJ_TRY(C, cudaMemcpyAsync(snode_d, snode.data(), snode.size() * 8, cudaMemcpyHostToDevice, st));
+  // kernel parameters
+  awc::AdjParams<T> A{};
+  A.ndim = p->ndim;
+  A.nx = (int32_t)p->nx;
+  A.ny = (int32_t)p->ny;
+  A.nz = (int32_t)V.nz;
+  A.halo = (int32_t)h;
+  A.px = V.px;
+  A.plane = V.px * p->ny;
+  const double d[3] = {p->dx, p->dy, p->ndim == 3 ? p->dz : 1.0};
+  for (int a = 0; a < 3; ++a) {
+    A.inv_d[a] = (T)(1.0 / d[a]);
+    A.inv_d2[a] = (T)(1.0 / (d[a] * d[a]));
+  }
+  A.F = (const T*)V.fact;
+  const T* cf = (const T*)V.coef;
+  const int64_t n3[3] = {p->nx, p->ny, V.nz};
+  for (int a = 0; a < p->ndim; ++a) {
+    const T* blk = cf + a * (8 * h + 4);
+    for (int s = 0; s < 2; ++s) {
+      A.a[a][s] = blk + s * h;
+      A.bK[a][s] = blk + 2 * h + s * h;
+      A.ah[a][s] = blk + 4 * h + s * (h + 1);
+      A.bKh[a][s] = blk + 4 * h + 2 * (h + 1) + s * (h + 1);
+      A.active[a][s] = V.active[a][s];
+      A.off[a][s] = s == 0 ? 0 : (int32_t)(n3[a] - h - 2);
+      A.mu[a][s] = mu[a][s];
+    }
+  }
+  const dim3 blk(32, 8);
+  const dim3 grid((unsigned)((p->nx - 2 + 31) / 32), (unsigned)((p->ny - 2 + 7) / 8),
+                  (unsigned)(p->ndim == 3 ? V.nz - 2 : 1));
+  // checkpoints and segment fields (gradient only)
+  const int64_t nseg = want_grad ? (nt + kchk - 1) / kchk : 0;
+  int64_t band_elems = 0;
+  for (int a = 0; a < p->ndim; ++a) band_elems += 2 * (V.psi_len[a] + V.xi_len[a]);
+  std::vector<T*> chk(nseg, nullptr);
+  std::vector<T*> seg;
+  if (want_grad) {
+    for (int64_t c = 0; c < nseg; ++c)
+      ADJ_TRY(C, mem.get(&chk[c], (3 * NP + band_elems) * sizeof(T)));
+    seg.resize(std::min<int64_t>(kchk, nt) + 2);
+    for (auto& sp : seg) ADJ_TRY(C, mem.get(&sp, fb));
+  }
+  auto save_or_restore = [&](T* base, int64_t s, bool save) -> int {
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+      return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st);
+    };
+    T* q = base;
+    for (int b = 0; b < 3; ++b, q += NP)
+      ADJ_TRY(C, save ? cp(q, V.buf[b], fb) : cp(V.buf[b], q, fb));
+    for (int a = 0; a < p->ndim; ++a)
+      for (int sd = 0; sd < 2; ++sd) {
+        void* ps = V.psi[a][sd][s & 1];
+        ADJ_TRY(C, save ? cp(q, ps, V.psi_len[a] * sizeof(T)) : cp(ps, q, V.psi_len[a] * sizeof(T)));
+        q += V.psi_len[a];
+        ADJ_TRY(C, save ? cp(q, V.xi[a][sd], V.xi_len[a] * sizeof(T))
+                        : cp(V.xi[a][sd], q, V.xi_len[a] * sizeof(T)));
+        q += V.xi_len[a];
+      }
+    return AWC_OK;
+  };
+  int rc;
+  if (want_grad) {
+    // forward run with checkpoints
+    if ((rc = awc_plan_reset(plan))) return rc;
+    for (int64_t c = 0; c < nseg; ++c) {
+      const int64_t s = c * kchk;
+      if ((rc = save_or_restore(chk[c], s, true))) return rc;
+      if ((rc = awc_plan_run(plan, std::min(kchk, nt - s), 1, nullptr))) return rc;
+    }
+  }
+  // backward
+  int i2 = 0, i3 = 1;  // lam[i2] = λ_{t+2}, lam[i3] = λ_{t+3}
+  int par = 0;         // nu[..][par] holds ν_{t+2}
+  for (int64_t c = (want_grad ? nseg : 1) - 1; c >= 0; --c) {
+    const int64_t s = want_grad ? c * kchk : 0, e = want_grad ? std::min(s + kchk, nt) : nt;
+    if (want_grad) {
+      // recompute p_{s-1} .. p_e of the segment
+      if ((rc = save_or_restore(chk[c], s, false))) return rc;
+      awc::plan_set_step(plan, s);
+      ADJ_TRY(C, cudaMemcpyAsync(seg[0], V.buf[s % 3], fb, cudaMemcpyDeviceToDevice, st));
+      ADJ_TRY(C, cudaMemcpyAsync(seg[1], V.buf[(s + 1) % 3], fb, cudaMemcpyDeviceToDevice, st));
+      for (int64_t t = s; t < e; ++t) {
+        if ((rc = awc_plan_run(plan, 1, 0, nullptr))) return rc;
+        ADJ_TRY(C, cudaMemcpyAsync(seg[t - s + 2], V.buf[(t + 2) % 3], fb, cudaMemcpyDeviceToDevice, st));
+      }
+    }
+    for (int64_t t = e - 1; t >= s; --t) {
+      // λ_{t+1} overwrites λ_{t+3}: adj_lambda reads λ_{t+3} only at the
+      // node it writes
+      T* ln = lam[i3];
+      A.lam2 = lam[i2];
+      A.lam3 = lam[i3];
+      A.lamn = ln;
+      for (int a = 0; a < p->ndim; ++a)
+        for (int sd = 0; sd < 2; ++sd) {
+          A.nu_old[a][sd] = nu[a][sd][par];
+          A.nu_new[a][sd] = nu[a][sd][par ^ 1];
+        }
+      awc::adj_lambda<T><<<grid, blk, 0, st>>>(A);
+      if (!RG.node.empty())
+        awc::adj_residuals<T><<<(unsigned)((RG.node.size() + 127) / 128), 128, 0, st>>>(
+            ln, rnode_d, roff_d, rids_d, (int32_t)RG.node.size(), res_d + t * nrec);
+      const T* pm1 = want_grad ? seg[t - s] : nullptr;
+      const T* p0 = want_grad ? seg[t - s + 1] : nullptr;
+      const T* pp1 = want_grad ? seg[t - s + 2] : nullptr;
+      awc::adj_nu_grad<T><<<grid, blk, 0, st>>>(A, pm1, p0, pp1, grad);
+      if (nsrc > 0)
+        awc::adj_sources<T><<<1, 32, 0, st>>>(ln, A.F, snode_d, (int32_t)nsrc, stf_d + t * nsrc,
+                                              grad, sout_d ? sout_d + t * nsrc : nullptr);
+      awc::adj_mu<T><<<grid, blk, 0, st>>>(A);
+      ADJ_TRY(C, cudaGetLastError());
+      std::swap(i2, i3);  // λ_{t+1} is the next step's λ_{t+2}
+      par ^= 1;
+    }
+  }
+  // outputs
+  if (want_grad) {
+    double* dense;
+    const int64_t N = p->nx * p->ny * V.nz;
+    ADJ_TRY(C, mem.get(&dense, N * sizeof(double)));
+    const int blocks = (int)std::min<int64_t>((N + 255) / 256, (int64_t)C->num_sms * 16);
+    awc::scale_unpitch<<<blocks, 256, 0, st>>>(grad, dense, N, p->nx, V.px, p->dt * p->dt);
+    ADJ_TRY(C, cudaGetLastError());
+    ADJ_TRY(C, cudaMemcpyAsync(grad_out, dense, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  }
+  if (src_out && nsrc > 0) {
+    double* sd;
+    ADJ_TRY(C, mem.get(&sd, nt * nsrc * sizeof(double)));
+    awc::to_double<T><<<(unsigned)std::min<int64_t>((nt * nsrc + 255) / 256, 4096), 256, 0, st>>>(
+        sout_d, sd, nt * nsrc);
+    ADJ_TRY(C, cudaGetLastError());
+    std::vector<double> tmp(nt * nsrc);
+    ADJ_TRY(C, cudaMemcpyAsync(tmp.data(), sd, tmp.size() * 8, cudaMemcpyDeviceToHost, st));
+    ADJ_TRY(C, cudaStreamSynchronize(st));
+    for (int64_t s2 = 0; s2 < nsrc; ++s2)
+      for (int64_t t = 0; t < nt; ++t) src_out[t + nt * s2] = tmp[t * nsrc + s2];
+  }
+  ADJ_TRY(C, cudaStreamSynchronize(st));
+  return AWC_OK;
+}
+
+int check_adjoint_problem(awc_ctx* C, const awc_problem* p) {
+  if (!p) return awc::fail(C, AWC_ERR_INVALID, "problem is NULL");
+  const int64_t n[3] = {p->nx, p->ny, p->ndim == 3 ? p->nz : 1};
+  for (int a = 0; a < p->ndim; ++a)
+    if (p->halo > 0 && n[a] < 2 * (int64_t)p->halo + 2)
+      return awc::fail(C, AWC_ERR_INVALID,
+                       "the adjoint needs non-overlapping CPML bands (n >= 2 halo + 2 per axis)");
+  return AWC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
+                        const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
+                        const int64_t* posrecs, const double* observed, int32_t checkpoint_every,
+                        double* misfit, double* grad_c2, double* traces) {
+  if (!ctx) return awc::fail(nullptr, AWC_ERR_INVALID, "ctx is NULL");
+  int rc;
+  if ((rc = check_adjoint_problem(ctx, p))) return rc;
+  if (!observed || !grad_c2 || !misfit)
+    return awc::fail(ctx, AWC_ERR_INVALID, "observed/grad_c2/misfit is NULL");
+  if (checkpoint_every < 1) return awc::fail(ctx, AWC_ERR_INVALID, "checkpoint_every must be >= 1");
+  awc_plan* plan = nullptr;
+  if ((rc = awc_plan_create(ctx, p, vel, coeffs, possrcs, dt2srctf, posrecs, &plan))) return rc;
+  // forward traces and residuals
+  const int64_t nt = p->nt, nrec = p->nrec;
+  std::vector<double> tr(std::max<int64_t>(nt * nrec, 1));
+  if ((rc = awc_plan_run(plan, nt, 1, nullptr)) || (nt * nrec > 0 && (rc = awc_plan_traces(plan, tr.data())))) {
+    awc_plan_destroy(plan);
+    return rc;
+  }
+  double J = 0.0;
+  std::vector<double> res(tr.size(), 0.0);
+  for (int64_t c = 0; c < nt * nrec; ++c) {
+    res[c] = tr[c] - observed[c];
+    J += 0.5 * res[c] * res[c];
+  }
+  *misfit = J;
+  if (traces && nt * nrec > 0) std::memcpy(traces, tr.data(), nt * nrec * sizeof(double));
+  rc = p->precision == AWC_F64
+           ? adjoint_impl<double>(ctx, plan, p, possrcs, dt2srctf, posrecs, res.data(),
+                                  checkpoint_every, grad_c2, nullptr)
+           : adjoint_impl<float>(ctx, plan, p, possrcs, dt2srctf, posrecs, res.data(),
+                                 checkpoint_every, grad_c2, nullptr);
+  awc_plan_destroy(plan);
+  return rc;
+}
+
+int awc_adjoint_sources(awc_ctx* ctx, const awc_problem* p, const double* vel,
+                        const double* coeffs, const int64_t* possrcs, const int64_t* posrecs,
+                        const double* adjoint_traces, double* src_out) {
+  if (!ctx) return awc::fail(nullptr, AWC_ERR_INVALID, "ctx is NULL");
+  int rc;
+  if ((rc = check_adjoint_problem(ctx, p))) return rc;
+  if (!adjoint_traces || !src_out)
+    return awc::fail(ctx, AWC_ERR_INVALID, "adjoint_traces/src_out is NULL");
+  awc_plan* plan = nullptr;
+  // the plan only provides fact and the coefficients; the injected values
+  // play no part in the transpose
+  std::vector<double> zero(std::max<int64_t>(p->nt * p->nsrc, 1), 0.0);
+  if ((rc = awc_plan_create(ctx, p, vel, coeffs, possrcs, zero.data(), posrecs, &plan))) return rc;
+  rc = p->precision == AWC_F64
+           ? adjoint_impl<double>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces, 1,
+                                  nullptr, src_out)
+           : adjoint_impl<float>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces, 1,
+                                 nullptr, src_out);
+  awc_plan_destroy(plan);
+  return rc;
+}
+
+}  // extern "C"

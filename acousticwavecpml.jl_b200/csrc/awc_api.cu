@@ -900,6 +900,39 @@ void record_error(const char* msg) { g_thread_err = msg; }
 int fail(awc_ctx* ctx, int code, const char* msg) {
   return set_err(ctx ? &ctx->err : nullptr, code, "%s", msg);
 }
+
+PlanView plan_view(awc_plan* P) {
+  PlanView V;
+  const awc_problem* p = &P->p;
+  V.ndim = p->ndim;
+  V.precision = p->precision;
+  V.halo = p->halo;
+  V.nx = p->nx;
+  V.ny = p->ny;
+  V.nz = p->ndim == 3 ? p->nz : 1;
+  V.px = P->px;
+  V.NP = P->NP;
+  V.nt = p->nt;
+  V.esz = P->esz;
+  for (int b = 0; b < 3; ++b) V.buf[b] = P->buf[b];
+  V.fact = P->fact;
+  for (int a = 0; a < p->ndim; ++a) {
+    V.psi_len[a] = (p->halo + 1) * cross_section(p, a);
+    V.xi_len[a] = p->halo * cross_section(p, a);
+    for (int sd = 0; sd < 2; ++sd) {
+      V.psi[a][sd][0] = P->psi[a][sd][0];
+      V.psi[a][sd][1] = P->psi[a][sd][1];
+      V.xi[a][sd] = P->xi[a][sd];
+      V.active[a][sd] = P->active[a][sd];
+    }
+  }
+  V.coef = P->coef;
+  V.traces = P->traces;
+  V.stream = P->ctx->stream;
+  return V;
+}
+
+void plan_set_step(awc_plan* P, int64_t step) { P->step = step; }
 }  // namespace awc
 
 // ---------------------------------------------------------------------------

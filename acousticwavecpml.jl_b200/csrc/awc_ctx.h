@@ -22,6 +22,27 @@ struct awc_ctx {
 };
 
 namespace awc {
+// The device state of a plan, for code outside the forward stepper (the
+// adjoint): step it reads pold = buf[it % 3], pcur = buf[(it + 1) % 3] and
+// writes pnew = buf[(it + 2) % 3]; ψ_old of step it is psi[axis][side][it & 1].
+struct PlanView {
+  int32_t ndim = 0, precision = 0, halo = 0;
+  int64_t nx = 0, ny = 0, nz = 1, px = 0, NP = 0, nt = 0;
+  size_t esz = 0;
+  void* buf[3] = {};
+  const void* fact = nullptr;
+  void* psi[3][2][2] = {};
+  void* xi[3][2] = {};
+  int64_t psi_len[3] = {}, xi_len[3] = {};  // elements of one side's array
+  const void* coef = nullptr;               // packed coefficients in the working precision
+  int32_t active[3][2] = {};
+  const void* traces = nullptr;             // device [nt][nrec]
+  cudaStream_t stream = nullptr;
+};
+PlanView plan_view(awc_plan* P);
+// Sets the step counter of a plan whose state was restored from a copy.
+void plan_set_step(awc_plan* P, int64_t step);
+
 // Sets the calling thread's last error (awc_last_error(NULL)) and, when ctx
 // is not NULL, the context's; returns code.
 int fail(awc_ctx* ctx, int code, const char* msg);

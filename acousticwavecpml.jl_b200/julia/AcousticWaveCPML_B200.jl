@@ -21,7 +21,7 @@ module AcousticWaveCPML_B200
 
 import ..AcousticWaveCPML: Sources, Receivers, calc_Kab_CPML
 
-export solve2D, solve3D
+export solve2D, solve3D, misfit, misfit_gradient
 
 const LIBAWCPML = get(ENV, "AWCPML_LIB", joinpath(@__DIR__, "..", "lib", "libawcpml.so"))
 
@@ -140,5 +140,74 @@ axis, free top at j = 1).
 """
 solve3D(lx::Real, ly::Real, lz::Real, lt::Real, vel::Array{<:Real,3}, srcs::Sources,
         recs::Receivers; kw...) = _solve((lx, ly, lz), lt, vel, srcs, recs; kw...)
+
+"""
+    misfit_gradient(ls, vel, srcs, recs, observed; dt, nt, halo=20, rcoef=0.0001,
+                    freetop=true, precision=:f64, checkpoint_every=50, device=0)
+
+Misfit J = 1/2 Σ (traces - observed)² of one shot (set up as in solve2D/solve3D,
+with a fixed `dt` and `nt`) and dJ/d(c²) per node, by the discrete adjoint in
+libawcpml (`awc_misfit_gradient`). No counterpart in the reference.
+"""
+function misfit_gradient(ls::NTuple{N,Real}, vel::Array{<:Real,N}, srcs::Sources,
+                         recs::Receivers, observed::Matrix{Float64}; dt::Real, nt::Integer,
+                         halo::Integer=20, rcoef::Real=0.0001, freetop::Bool=true,
+                         precision::Symbol=:f64, checkpoint_every::Integer=50,
+                         device::Integer=0) where {N}
+    f0 = srcs.freqdomain
+    vel_max = maximum(vel)
+    ns = size(vel)
+    ds = ntuple(a -> ls[a] / (ns[a] - 1), N)
+    times = collect(range(0.0, step=dt, length=nt))
+    dt2srctf = zeros(nt, srcs.n)
+    for s = 1:srcs.n
+        dt2srctf[:, s] .= (dt^2 / prod(ds)) .* srcs.srctfs[s].(times, srcs.t0s[s], f0)
+    end
+    snap(pos) = round.(Int64, pos ./ reshape(collect(ds), 1, N) .+ 1, RoundNearestTiesUp)
+    possrcs, posrecs = snap(srcs.positions), snap(recs.positions)
+    coeffs = packed_coeffs(halo, dt, ds, vel_max, rcoef, f0, freetop)
+    prob = AwcProblem(Int32(N), precision == :f32 ? AWC_F32 : AWC_F64, ns[1], ns[2],
+                      N == 3 ? ns[3] : 1, Int32(halo), Int32(freetop), ds[1], ds[2],
+                      N == 3 ? ds[3] : 1.0, Float64(dt), nt, srcs.n, recs.n)
+    J = Ref{Float64}(0.0)
+    grad = zeros(Float64, ns)
+    traces = zeros(Float64, nt, recs.n)
+    ctx = context(device)
+    rc = ccall((:awc_misfit_gradient, LIBAWCPML), Cint,
+               (Ptr{Cvoid}, Ref{AwcProblem}, Ptr{Float64}, Ptr{Float64}, Ptr{Int64},
+                Ptr{Float64}, Ptr{Int64}, Ptr{Float64}, Int32, Ref{Float64}, Ptr{Float64},
+                Ptr{Float64}),
+               ctx, prob, Array{Float64}(vel), coeffs, possrcs, dt2srctf, posrecs, observed,
+               Int32(checkpoint_every), J, grad, traces)
+    check(rc, ctx)
+    recs.seismograms = traces
+    return J[], grad
+end
+
+"""
+    misfit(c2, ls, srcs, recs, observed; kw...)
+
+J as a function of c² (the squared velocity). With ChainRulesCore loaded, its
+rrule returns dJ/d(c²) from the adjoint, so Zygote and friends differentiate
+through the solver.
+"""
+misfit(c2::Array{<:Real,N}, ls::NTuple{N,Real}, srcs::Sources, recs::Receivers,
+       observed::Matrix{Float64}; kw...) where {N} =
+    misfit_gradient(ls, sqrt.(c2), srcs, recs, observed; kw...)[1]
+
+try
+    @eval import ChainRulesCore
+catch
+end
+if isdefined(@__MODULE__, :ChainRulesCore)
+    @eval function ChainRulesCore.rrule(::typeof(misfit), c2::Array{<:Real,N}, ls::NTuple{N,Real},
+                                        srcs::Sources, recs::Receivers,
+                                        observed::Matrix{Float64}; kw...) where {N}
+        J, g = misfit_gradient(ls, sqrt.(c2), srcs, recs, observed; kw...)
+        nt = ChainRulesCore.NoTangent()
+        misfit_pullback(ΔJ) = (nt, ChainRulesCore.unthunk(ΔJ) .* g, nt, nt, nt, nt)
+        return J, misfit_pullback
+    end
+end
 
 end # module

@@ -204,6 +204,32 @@ int awc_forward_batch(awc_ctx* ctx, int32_t nmodels, const awc_problem* models,
                       const double* const* vel, int32_t nshots, const awc_shot* shots,
                       double* const* traces);
 
+/* ---- Adjoint ---------------------------------------------------------------
+ * No counterpart in the reference, which has no gradient. Both entry points
+ * run the exact discrete transpose of the time step above (awc_forward's
+ * arithmetic for fixed c), backwards in time, on the interior nodes. They
+ * need CPML bands that do not overlap (n >= 2 halo + 2 on each axis) and
+ * allocate their working memory for the duration of the call.
+ *
+ * awc_misfit_gradient: J = 1/2 Σ_t Σ_r (traces[t,r] - observed[t,r])² of the
+ * shot described like awc_forward, and dJ/d(c²) per node (nx*ny[*nz],
+ * column-major, 0 on the rim). The forward state is saved every
+ * `checkpoint_every` steps and each segment is recomputed once during the
+ * backward pass (memory: nt / checkpoint_every saved states plus
+ * checkpoint_every + 2 pressure fields). `traces` (nt x nrec) may be NULL. */
+int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
+                        const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
+                        const int64_t* posrecs, const double* observed, int32_t checkpoint_every,
+                        double* misfit, double* grad_c2, double* traces);
+
+/* The transpose of the linear map from injected source values (dt2srctf,
+ * nt x nsrc) to traces (nt x nrec) for fixed c: src_out (nt x nsrc) =
+ * Aᵀ adjoint_traces. Sources and receivers on the Dirichlet rim have no
+ * adjoint (their entries are 0). */
+int awc_adjoint_sources(awc_ctx* ctx, const awc_problem* p, const double* vel,
+                        const double* coeffs, const int64_t* possrcs, const int64_t* posrecs,
+                        const double* adjoint_traces, double* src_out);
+
 /* awc_forward for 2D FP32 problems without any device memory allocation.
  * No counterpart in the reference (its solvers always allocate).
  *

@@ -1,0 +1,147 @@
+"""Discrete adjoint (awc_misfit_gradient, awc_adjoint_sources) on the GPU.
+
+* Dot-product test of the transpose of the source-to-trace map:
+  <A s, r> = <s, Aᵀ r> to 1e-12 relative (FP64), 2D and 3D, with sources and
+  receivers inside and outside the CPML bands.
+* Gradient dJ/d(c²) against central finite differences of the FP64 oracle
+  forward (eps = 1e-4 relative, 20 cells in 2D, 10 in 3D, dt fixed), 1e-6.
+* The checkpoint interval does not change the gradient (bitwise); the FP32
+  gradient follows the FP64 one (relative L2 <= 2e-3)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def model2d(rng, nx=60, ny=50, d=10.0, freetop=True, halo=8):
+    vel = 2000.0 + 8.0 * np.arange(ny)[None, :] + 100.0 * rng.random((nx, ny))
+    L = ((nx - 1) * d, (ny - 1) * d)
+    srcs = [[(nx // 2) * d, 6 * d], [3 * d, 20 * d]]  # one inside the x band
+    recs = [[(i - 1) * d, 4 * d] for i in range(4, nx - 3, 5)] + [[(nx - 4) * d, (ny - 5) * d]]
+    return L, vel, srcs, recs, dict(halo=halo, rcoef=1e-4, freetop=freetop)
+
+
+def model3d(rng, n=(40, 36, 34), d=10.0, freetop=True, halo=6):
+    nx, ny, nz = n
+    vel = 2000.0 + 10.0 * np.arange(ny)[None, :, None] + 100.0 * rng.random(n)
+    L = ((nx - 1) * d, (ny - 1) * d, (nz - 1) * d)
+    srcs = [[(nx // 2) * d, 8 * d, (nz // 2) * d], [3 * d, 12 * d, 4 * d]]
+    recs = [[(i - 1) * d, 3 * d, (k - 1) * d] for i in (4, nx // 2, nx - 3) for k in (5, nz - 4)]
+    recs += [[(nx // 3) * d, (ny - 4) * d, (nz // 3) * d]]
+    return L, vel, srcs, recs, dict(halo=halo, rcoef=1e-4, freetop=freetop)
+
+
+def setup(pkg, L, vel, srcs, recs, kw, precision="f64", nt=None, lt=0.15, f0=12.0):
+    S = pkg.Sources(srcs, [0.05] * len(srcs), [pkg.rickersource1D] * len(srcs), f0)
+    R = pkg.Receivers(recs)
+    return pkg.prepare(L, lt, vel, S, R, precision=precision, ppw=1e-9, nt=nt, **kw)
+
+
+def traces_of(ctx, s):
+    p = s["problem"]
+    tr = np.zeros((p.nt, p.nrec), order="F")
+    ctx.forward(p, s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"], s["posrecs"], tr)
+    return tr
+
+
+@pytest.mark.parametrize("dim,freetop", [(2, True), (2, False), (3, True), (3, False)])
+def test_dot_product(pkg, ctx, dim, freetop):
+    from acousticwavecpml_b200 import adjoint
+    rng = np.random.default_rng(3 + dim)
+    L, vel, srcs, recs, kw = (model2d if dim == 2 else model3d)(rng, freetop=freetop)
+    s = setup(pkg, L, vel, srcs, recs, kw)
+    p = s["problem"]
+    sa = rng.standard_normal((p.nt, p.nsrc))
+    r = rng.standard_normal((p.nt, p.nrec))
+    s2 = dict(s, dt2srctf=np.asfortranarray(sa))
+    lhs = float(np.sum(traces_of(ctx, s2) * r))
+    rhs = float(np.sum(sa * adjoint.adjoint_sources(s, r, ctx)))
+    print(f"dot {dim}D freetop={freetop}: {lhs:.15e} {rhs:.15e}")
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs))
+
+
+def _fd_cells(rng, vel, halo, n):
+    shape = vel.shape
+    cells = []
+    vmax = vel.max()
+    while len(cells) < n:
+        c = tuple(int(rng.integers(1, m - 1)) for m in shape)
+        if vel[c] < 0.99 * vmax and c not in cells:
+            cells.append(c)
+    return cells
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_gradient_vs_oracle_fd(pkg, oracle, ctx, dim):
+    from acousticwavecpml_b200 import adjoint
+    rng = np.random.default_rng(11 + dim)
+    L, vel, srcs, recs, kw = (model2d if dim == 2 else model3d)(rng)
+    s = setup(pkg, L, vel, srcs, recs, kw)
+    p = s["problem"]
+    # observed data: a smoother model's traces
+    s_obs = dict(s, vel=np.asfortranarray(np.full_like(vel, vel.mean())))
+    obs = traces_of(ctx, s_obs)
+    J, grad, traces = adjoint.misfit_gradient(s, obs, checkpoint_every=17, ctx=ctx)
+    assert abs(J - 0.5 * np.sum((traces - obs) ** 2)) <= 1e-12 * J
+
+    def oracle_J(v):
+        so = oracle.setup(L, None, v, srcs, [0.05] * len(srcs), 12.0, recs, check_ppw=False,
+                          dt=s["dt"], nt=p.nt, **kw)
+        so["coeffs"] = s["coeffs"]  # fixed CPML profile (it depends on max(vel))
+        _, tr = oracle.forward(so)
+        return 0.5 * np.sum((tr - obs) ** 2)
+
+    c2 = vel ** 2
+    for cell in _fd_cells(rng, vel, kw["halo"], 20 if dim == 2 else 10):
+        eps = 1e-4 * c2[cell]
+        vp, vm = vel.copy(), vel.copy()
+        vp[cell] = np.sqrt(c2[cell] + eps)
+        vm[cell] = np.sqrt(c2[cell] - eps)
+        fd = (oracle_J(vp) - oracle_J(vm)) / (2 * eps)
+        print(f"{dim}D cell {cell}: adjoint {grad[cell]:.10e} fd {fd:.10e}")
+        assert abs(grad[cell] - fd) <= 1e-6 * max(abs(fd), 1e-3 * np.abs(grad).max())
+
+
+def test_checkpoint_interval_is_exact(pkg, ctx):
+    from acousticwavecpml_b200 import adjoint
+    rng = np.random.default_rng(5)
+    L, vel, srcs, recs, kw = model3d(rng, freetop=False)
+    s = setup(pkg, L, vel, srcs, recs, kw, nt=90)
+    obs = np.zeros((90, s["problem"].nrec))
+    ref = adjoint.misfit_gradient(s, obs, checkpoint_every=90, ctx=ctx)[1]
+    for k in (1, 7, 50):
+        g = adjoint.misfit_gradient(s, obs, checkpoint_every=k, ctx=ctx)[1]
+        assert np.array_equal(g, ref), k
+    assert np.abs(ref).max() > 0
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_fp32_gradient_follows_fp64(pkg, ctx, dim):
+    from acousticwavecpml_b200 import adjoint
+    rng = np.random.default_rng(21 + dim)
+    L, vel, srcs, recs, kw = (model2d if dim == 2 else model3d)(rng)
+    s64 = setup(pkg, L, vel, srcs, recs, kw, "f64")
+    s32 = setup(pkg, L, vel, srcs, recs, kw, "f32", nt=s64["nt"])
+    s32["dt2srctf"] = s64["dt2srctf"]
+    obs = traces_of(ctx, dict(s64, vel=np.asfortranarray(np.full_like(vel, vel.mean()))))
+    J64, g64, _ = adjoint.misfit_gradient(s64, obs, 25, ctx)
+    J32, g32, _ = adjoint.misfit_gradient(s32, obs, 25, ctx)
+    e = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
+    print(f"{dim}D fp32 gradient rel-L2 {e:.3e}, misfit {J32:.6e} vs {J64:.6e}")
+    assert e <= 2e-3
+    assert abs(J32 - J64) <= 1e-4 * J64
+
+
+def test_torch_autograd_function(pkg, ctx):
+    import torch
+    from acousticwavecpml_b200 import adjoint
+    rng = np.random.default_rng(8)
+    L, vel, srcs, recs, kw = model2d(rng)
+    s = setup(pkg, L, vel, srcs, recs, kw)
+    obs = traces_of(ctx, dict(s, vel=np.asfortranarray(np.full_like(vel, vel.mean()))))
+    c2 = torch.tensor(vel ** 2, dtype=torch.float64, requires_grad=True)
+    J = adjoint.C2Misfit.apply(c2, s, obs, 20)
+    J.backward()
+    Jr, gr, _ = adjoint.misfit_gradient(s, obs, 20, ctx)
+    assert abs(J.item() - Jr) <= 1e-12 * Jr
+    assert np.allclose(c2.grad.numpy(), gr, rtol=0, atol=1e-12 * np.abs(gr).max())
