@@ -55,9 +55,10 @@ struct AdjParams {
   int64_t px, plane;
   T inv_d[3], inv_d2[3];
   const T* F;
+  const T* G;     // F λ_{t+2} on the interior, 0 on the rim
   const T* lam2;  // λ_{t+2}
   const T* lam3;  // λ_{t+3}
-  T* lamn;        // λ_{t+1}
+  T* lamn;        // λ_{t+1} (may alias lam3: read and written at the same node)
   T* mu[3][2];    // μ, updated in place (layout of ψ)
   const T* nu_old[3][2];  // ν_{t+2} (layout of ξ)
   T* nu_new[3][2];        // ν_{t+1}
@@ -80,19 +81,11 @@ __device__ __forceinline__ int64_t band_index(const AdjParams<T>& A, int a, int 
   return i + A.px * (j + (int64_t)A.ny * e);
 }
 
+// a ν_{t+2} of axis a at the node whose axis coordinate is c (other
+// coordinates i, j, k), when it is a band node of that axis.
 template <typename T>
-__device__ __forceinline__ bool interior(const AdjParams<T>& A, int i, int j, int k) {
-  return i >= 1 && i <= A.nx - 2 && j >= 1 && j <= A.ny - 2 &&
-         (A.ndim == 2 || (k >= 1 && k <= A.nz - 2));
-}
-
-// F λ_{t+2} + a ν_{t+2} of axis a at node (i, j, k), 0 off the interior.
-template <typename T>
-__device__ __forceinline__ T adj_g(const AdjParams<T>& A, int a, int i, int j, int k) {
-  if (!interior(A, i, j, k)) return T(0);
-  const int64_t o = i + A.px * j + A.plane * k;
-  T g = A.F[o] * A.lam2[o];
-  const int c = a == 0 ? i : a == 1 ? j : k;
+__device__ __forceinline__ T adj_anu(const AdjParams<T>& A, int a, int c, int i, int j, int k) {
+  T g = 0;
   for (int s = 0; s < 2; ++s) {
     if (!A.active[a][s]) continue;
     const int q = c - A.off[a][s];
@@ -102,32 +95,57 @@ __device__ __forceinline__ T adj_g(const AdjParams<T>& A, int a, int i, int j, i
   return g;
 }
 
-// λ_{t+1} without the receiver residuals.
+// Whether axis coordinate c lies within one node of a band (of any side).
+template <typename T>
+__device__ __forceinline__ bool adj_band_near(const AdjParams<T>& A, int c, int n) {
+  return A.halo > 0 && (c <= A.halo + 1 || c >= n - A.halo - 2);
+}
+
+// The band part of λ_{t+1} along axis a at node (i, j, k) whose axis
+// coordinate is c: the transposed stencil of a ν_{t+2} and the ψ-face terms,
+// non-zero only within one node of a band.
+template <typename T>
+__device__ __forceinline__ T adj_band_terms(const AdjParams<T>& A, int a, int c, int n, int i,
+                                            int j, int k) {
+  if (A.halo == 0 || (c > A.halo + 1 && c < n - A.halo - 2)) return T(0);
+  const int di = a == 0, dj = a == 1, dk = a == 2;
+  T acc = T(-2) * adj_anu(A, a, c, i, j, k);
+  if (c + 1 <= n - 2) acc += adj_anu(A, a, c + 1, i + di, j + dj, k + dk);
+  if (c - 1 >= 1) acc += adj_anu(A, a, c - 1, i - di, j - dj, k - dk);
+  T r = A.inv_d2[a] * acc;
+  for (int s = 0; s < 2; ++s) {
+    if (!A.active[a][s]) continue;
+    const int e1 = c - 1 - A.off[a][s], e2 = c - A.off[a][s];
+    T f = 0;
+    if (e1 >= 0 && e1 <= A.halo)
+      f += A.ah[a][s][e1] * A.mu[a][s][band_index(A, a, A.halo + 1, e1, i, j, k)];
+    if (e2 >= 0 && e2 <= A.halo)
+      f -= A.ah[a][s][e2] * A.mu[a][s][band_index(A, a, A.halo + 1, e2, i, j, k)];
+    r += A.inv_d[a] * f;
+  }
+  return r;
+}
+
+// λ_{t+1} without the receiver residuals: 2 λ_{t+2} - λ_{t+3} plus the
+// transposed stencil of G = F λ_{t+2} and the band terms; one thread per
+// node.
 template <typename T>
 __global__ void __launch_bounds__(256) adj_lambda(AdjParams<T> A) {
   const int i = 1 + blockIdx.x * 32 + threadIdx.x;
   const int j = 1 + blockIdx.y * 8 + threadIdx.y;
   const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
   if (i > A.nx - 2 || j > A.ny - 2) return;
-  const int64_t o = i + A.px * j + A.plane * k;
-  T lam = T(2) * A.lam2[o] - A.lam3[o];
-  for (int a = 0; a < A.ndim; ++a) {
-    const int di = a == 0, dj = a == 1, dk = a == 2;
-    const T gm = adj_g(A, a, i - di, j - dj, k - dk);
-    const T g0 = adj_g(A, a, i, j, k);
-    const T gp = adj_g(A, a, i + di, j + dj, k + dk);
-    lam += A.inv_d2[a] * (gp - T(2) * g0 + gm);
-    const int c = a == 0 ? i : a == 1 ? j : k;
-    for (int s = 0; s < 2; ++s) {
-      if (!A.active[a][s]) continue;
-      const int e1 = c - 1 - A.off[a][s], e2 = c - A.off[a][s];
-      if (e1 >= 0 && e1 <= A.halo)
-        lam += A.inv_d[a] * A.ah[a][s][e1] *
-               A.mu[a][s][band_index(A, a, A.halo + 1, e1, i, j, k)];
-      if (e2 >= 0 && e2 <= A.halo)
-        lam -= A.inv_d[a] * A.ah[a][s][e2] *
-               A.mu[a][s][band_index(A, a, A.halo + 1, e2, i, j, k)];
-    }
+  const int64_t px = A.px, plane = A.plane;
+  const int64_t o = i + px * j + plane * k;
+  const T gc = __ldg(A.G + o);
+  T lam = T(2) * __ldg(A.lam2 + o) - A.lam3[o];
+  lam += A.inv_d2[0] * (__ldg(A.G + o + 1) - T(2) * gc + __ldg(A.G + o - 1)) +
+         A.inv_d2[1] * (__ldg(A.G + o + px) - T(2) * gc + __ldg(A.G + o - px));
+  if (adj_band_near(A, i, A.nx)) lam += adj_band_terms(A, 0, i, A.nx, i, j, k);
+  if (adj_band_near(A, j, A.ny)) lam += adj_band_terms(A, 1, j, A.ny, i, j, k);
+  if (A.ndim == 3) {
+    lam += A.inv_d2[2] * (__ldg(A.G + o + plane) - T(2) * gc + __ldg(A.G + o - plane));
+    if (adj_band_near(A, k, A.nz)) lam += adj_band_terms(A, 2, k, A.nz, i, j, k);
   }
   A.lamn[o] = lam;
 }
@@ -145,70 +163,82 @@ __global__ void adj_residuals(T* __restrict__ lamn, const int64_t* __restrict__ 
   lamn[node[n]] = v;
 }
 
-// ν_{t+1} and the gradient accumulation dJ/dF += λ_{t+1} (p_{t+1} - 2 p_t +
-// p_{t-1}) / F (the source term is removed by adj_sources).
+// G = F λ_{t+1} for the next step, and the gradient accumulation
+// dJ/dF += λ_{t+1} (p_{t+1} - 2 p_t + p_{t-1}) / F (the source term is
+// removed by adj_sources).
 template <typename T>
-__global__ void __launch_bounds__(256) adj_nu_grad(AdjParams<T> A, const T* __restrict__ pm1,
-                                                   const T* __restrict__ p0,
-                                                   const T* __restrict__ pp1,
-                                                   double* __restrict__ grad) {
+__global__ void __launch_bounds__(256) adj_grad(AdjParams<T> A, T* __restrict__ Gn,
+                                                const T* __restrict__ pm1,
+                                                const T* __restrict__ p0,
+                                                const T* __restrict__ pp1,
+                                                double* __restrict__ grad) {
   const int i = 1 + blockIdx.x * 32 + threadIdx.x;
   const int j = 1 + blockIdx.y * 8 + threadIdx.y;
   const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
   if (i > A.nx - 2 || j > A.ny - 2) return;
   const int64_t o = i + A.px * j + A.plane * k;
   const T lam = A.lamn[o], f = A.F[o];
-  for (int a = 0; a < A.ndim; ++a) {
-    const int c = a == 0 ? i : a == 1 ? j : k;
-    for (int s = 0; s < 2; ++s) {
-      if (!A.active[a][s]) continue;
-      const int q = c - A.off[a][s];
-      if (q < 1 || q > A.halo) continue;
-      const int64_t x = band_index(A, a, A.halo, q - 1, i, j, k);
-      A.nu_new[a][s][x] = A.bK[a][s][q - 1] * A.nu_old[a][s][x] + f * lam;
-    }
-  }
+  Gn[o] = f * lam;
   if (grad) {
     const double b = ((double)pp1[o] - 2.0 * (double)p0[o] + (double)pm1[o]) / (double)f;
     grad[o] += (double)lam * b;
   }
 }
 
-// μ_{t+1} in place: band node q updates face q, the first node also face 0.
+// ν_{t+1} and μ_{t+1} of one axis side, one thread per band node (entry q,
+// other coordinates): ν_{t+1}[q-1] = bK ν_{t+2}[q-1] + F λ_{t+1}; face q
+// (and face 0 for q = 1) of μ in place, with w of node q+1 formed from
+// ν_{t+2} so that no thread reads another's new ν.
 template <typename T>
-__global__ void __launch_bounds__(256) adj_mu(AdjParams<T> A) {
-  const int i = 1 + blockIdx.x * 32 + threadIdx.x;
-  const int j = 1 + blockIdx.y * 8 + threadIdx.y;
-  const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
-  if (i > A.nx - 2 || j > A.ny - 2) return;
-  const int64_t o = i + A.px * j + A.plane * k;
-  for (int a = 0; a < A.ndim; ++a) {
-    const int c = a == 0 ? i : a == 1 ? j : k;
+__global__ void __launch_bounds__(256) adj_band(AdjParams<T> A, int a, int s, int64_t count) {
+  const int h = A.halo;
+  const int n1 = a == 0 ? A.ny - 2 : A.nx - 2;        // fastest other coordinate count
+  const int n2 = a == 2 ? A.ny - 2 : (A.ndim == 3 ? A.nz - 2 : 1);
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int q, u, v;
+    if (a == 0) {  // q fastest: ψ_x is contiguous in q
+      q = 1 + (int)(t % h);
+      u = (int)((t / h) % n1);
+      v = (int)(t / ((int64_t)h * n1));
+    } else {       // x fastest
+      u = (int)(t % n1);
+      q = 1 + (int)((t / n1) % h);
+      v = (int)(t / ((int64_t)n1 * h));
+    }
+    (void)n2;
+    const int c = q + A.off[a][s];
+    int i, j, k;
+    if (a == 0) { i = c; j = 1 + u; k = A.ndim == 3 ? 1 + v : 0; }
+    else if (a == 1) { i = 1 + u; j = c; k = A.ndim == 3 ? 1 + v : 0; }
+    else { i = 1 + u; j = 1 + v; k = c; }
     const int64_t step = a == 0 ? 1 : a == 1 ? A.px : A.plane;
-    const int di = a == 0, dj = a == 1, dk = a == 2;
-    for (int s = 0; s < 2; ++s) {
-      if (!A.active[a][s]) continue;
-      const int q = c - A.off[a][s];
-      if (q < 1 || q > A.halo) continue;
-      const T wq = A.a[a][s][q - 1] * A.nu_new[a][s][band_index(A, a, A.halo, q - 1, i, j, k)] +
-                   A.F[o] * A.lamn[o];
-      T wn = 0;
-      if (q + 1 <= A.halo)
-        wn = A.a[a][s][q] * A.nu_new[a][s][band_index(A, a, A.halo, q, i + di, j + dj, k + dk)] +
-             A.F[o + step] * A.lamn[o + step];
-      const int64_t m = band_index(A, a, A.halo + 1, q, i, j, k);
-      A.mu[a][s][m] = A.bKh[a][s][q] * A.mu[a][s][m] + A.inv_d[a] * (wq - wn);
-      if (q == 1) {
-        const int64_t m0 = band_index(A, a, A.halo + 1, 0, i, j, k);
-        A.mu[a][s][m0] = A.bKh[a][s][0] * A.mu[a][s][m0] - A.inv_d[a] * wq;
-      }
+    const int64_t o = i + A.px * j + A.plane * k;
+    const T flam = A.F[o] * A.lamn[o];
+    const int64_t x = band_index(A, a, h, q - 1, i, j, k);
+    const T nu_n = A.bK[a][s][q - 1] * A.nu_old[a][s][x] + flam;
+    A.nu_new[a][s][x] = nu_n;
+    const T wq = A.a[a][s][q - 1] * nu_n + flam;
+    T wn = 0;
+    if (q + 1 <= h) {
+      const int di = a == 0, dj = a == 1, dk = a == 2;
+      const T flam1 = A.F[o + step] * A.lamn[o + step];
+      const T nu1 = A.bK[a][s][q] * A.nu_old[a][s][band_index(A, a, h, q, i + di, j + dj, k + dk)] +
+                    flam1;
+      wn = A.a[a][s][q] * nu1 + flam1;
+    }
+    const int64_t m = band_index(A, a, h + 1, q, i, j, k);
+    A.mu[a][s][m] = A.bKh[a][s][q] * A.mu[a][s][m] + A.inv_d[a] * (wq - wn);
+    if (q == 1) {
+      const int64_t m0 = band_index(A, a, h + 1, 0, i, j, k);
+      A.mu[a][s][m0] = A.bKh[a][s][0] * A.mu[a][s][m0] - A.inv_d[a] * wq;
     }
   }
 }
 
-// Per source (one thread each, serial over sources for a fixed summation
-// order): the adjoint of the injected value, λ_{t+1} at the source node,
-// and the removal of the source term from the gradient bracket.
+// Per source (one thread, serial over sources for a fixed summation order):
+// the adjoint of the injected value, λ_{t+1} at the source node, and the
+// removal of the source term from the gradient bracket.
 template <typename T>
 __global__ void adj_sources(const T* __restrict__ lamn, const T* __restrict__ F,
                             const int64_t* __restrict__ node, int32_t nsrc,
@@ -305,9 +335,13 @@ Groups group_nodes(const awc_problem* p, int64_t px, const int64_t* pos, int64_t
 }
 
 template <typename T>
+// Gradient mode (grad_out set): the checkpointed forward run gives the
+// traces, the misfit against `observed` and the residuals. Transpose mode
+// (src_out set): `residual` are the adjoint traces.
 int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t* possrcs,
                  const double* dt2srctf, const int64_t* posrecs, const double* residual,
-                 int64_t kchk, double* grad_out, double* src_out) {
+                 const double* observed, double* misfit, double* traces_out, int64_t kchk,
+                 double* grad_out, double* src_out) {
   const awc::PlanView V = awc::plan_view(plan);
   cudaStream_t st = V.stream;
   const int64_t nt = p->nt, nsrc = p->nsrc, nrec = p->nrec, h = p->halo;
@@ -315,8 +349,12 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
   const bool want_grad = grad_out != nullptr;
   DevMem mem;
   // adjoint fields
-  T *lam[2], *mu[3][2] = {}, *nu[3][2][2] = {};
-  for (int b = 0; b < 2; ++b) ADJ_TRY(C, mem.get(&lam[b], fb));
+  T *lam[2], *G[2], *mu[3][2] = {}, *nu[3][2][2] = {};
+  for (int b = 0; b < 2; ++b) {
+    ADJ_TRY(C, mem.get(&lam[b], fb));
+    ADJ_TRY(C, mem.get(&G[b], fb));
+    ADJ_TRY(C, cudaMemsetAsync(G[b], 0, fb, st));
+  }
   for (int a = 0; a < p->ndim; ++a)
     for (int s = 0; s < 2; ++s) {
       ADJ_TRY(C, mem.get(&mu[a][s], V.psi_len[a] * sizeof(T)));
@@ -332,13 +370,10 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
     ADJ_TRY(C, mem.get(&grad, NP * sizeof(double)));
     ADJ_TRY(C, cudaMemsetAsync(grad, 0, NP * sizeof(double), st));
   }
-  // residual rows [nt][nrec] and source rows [nt][nsrc] in T
+  // source rows [nt][nsrc] in T (the residual rows follow the forward run)
   std::vector<T> rows(std::max<int64_t>(nt * nrec, 1));
-  for (int64_t r = 0; r < nrec; ++r)
-    for (int64_t t = 0; t < nt; ++t) rows[t * nrec + r] = (T)residual[t + nt * r];
   T* res_d;
   ADJ_TRY(C, mem.get(&res_d, rows.size() * sizeof(T)));
-  ADJ_TRY(C, cudaMemcpyAsync(res_d, rows.data(), rows.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   std::vector<T> srows(std::max<int64_t>(nt * nsrc, 1), T(0));
   if (dt2srctf)
     for (int64_t s = 0; s < nsrc; ++s)
@@ -405,10 +440,13 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
   std::vector<T*> chk(nseg, nullptr);
   std::vector<T*> seg;
   if (want_grad) {
-    for (int64_t c = 0; c < nseg; ++c)
-      ADJ_TRY(C, mem.get(&chk[c], (3 * NP + band_elems) * sizeof(T)));
+    // one allocation for the saved states and the segment's fields
+    const int64_t chk_elems = (3 * NP + band_elems + 63) / 64 * 64;
     seg.resize(std::min<int64_t>(kchk, nt) + 2);
-    for (auto& sp : seg) ADJ_TRY(C, mem.get(&sp, fb));
+    T* arena;
+    ADJ_TRY(C, mem.get(&arena, (nseg * chk_elems + (int64_t)seg.size() * NP) * sizeof(T)));
+    for (int64_t c = 0; c < nseg; ++c) chk[c] = arena + c * chk_elems;
+    for (size_t m = 0; m < seg.size(); ++m) seg[m] = arena + nseg * chk_elems + (int64_t)m * NP;
   }
   auto save_or_restore = [&](T* base, int64_t s, bool save) -> int {
     auto cp = [&](void* dst, const void* src, size_t bytes) {
@@ -429,17 +467,32 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
     return AWC_OK;
   };
   int rc;
+  std::vector<double> res_h;
   if (want_grad) {
-    // forward run with checkpoints
+    // forward run with checkpoints, then the traces, misfit and residuals
     if ((rc = awc_plan_reset(plan))) return rc;
     for (int64_t c = 0; c < nseg; ++c) {
       const int64_t s = c * kchk;
       if ((rc = save_or_restore(chk[c], s, true))) return rc;
-      if ((rc = awc_plan_run(plan, std::min(kchk, nt - s), 1, nullptr))) return rc;
+      if ((rc = awc_plan_run(plan, std::min(kchk, nt - s), 0, nullptr))) return rc;
     }
+    res_h.assign(std::max<int64_t>(nt * nrec, 1), 0.0);
+    if (nt * nrec > 0 && (rc = awc_plan_traces(plan, res_h.data()))) return rc;
+    if (traces_out && nt * nrec > 0) std::memcpy(traces_out, res_h.data(), nt * nrec * sizeof(double));
+    double J = 0.0;
+    for (int64_t c = 0; c < nt * nrec; ++c) {
+      res_h[c] -= observed[c];
+      J += 0.5 * res_h[c] * res_h[c];
+    }
+    *misfit = J;
+    residual = res_h.data();
   }
+  for (int64_t r = 0; r < nrec; ++r)
+    for (int64_t t = 0; t < nt; ++t) rows[t * nrec + r] = (T)residual[t + nt * r];
+  ADJ_TRY(C, cudaMemcpyAsync(res_d, rows.data(), rows.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   // backward
   int i2 = 0, i3 = 1;  // lam[i2] = λ_{t+2}, lam[i3] = λ_{t+3}
+  int gi = 0;          // G[gi] = F λ_{t+2}
   int par = 0;         // nu[..][par] holds ν_{t+2}
   for (int64_t c = (want_grad ? nseg : 1) - 1; c >= 0; --c) {
     const int64_t s = want_grad ? c * kchk : 0, e = want_grad ? std::min(s + kchk, nt) : nt;
@@ -449,10 +502,10 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       awc::plan_set_step(plan, s);
       ADJ_TRY(C, cudaMemcpyAsync(seg[0], V.buf[s % 3], fb, cudaMemcpyDeviceToDevice, st));
       ADJ_TRY(C, cudaMemcpyAsync(seg[1], V.buf[(s + 1) % 3], fb, cudaMemcpyDeviceToDevice, st));
-      for (int64_t t = s; t < e; ++t) {
-        if ((rc = awc_plan_run(plan, 1, 0, nullptr))) return rc;
-        ADJ_TRY(C, cudaMemcpyAsync(seg[t - s + 2], V.buf[(t + 2) % 3], fb, cudaMemcpyDeviceToDevice, st));
-      }
+      awc::plan_keep_fields(plan, (void* const*)(seg.data() + 2), s, e - s);
+      rc = awc_plan_run(plan, e - s, 0, nullptr);
+      awc::plan_keep_fields(plan, nullptr, 0, 0);
+      if (rc) return rc;
     }
     for (int64_t t = e - 1; t >= s; --t) {
       // λ_{t+1} overwrites λ_{t+3}: adj_lambda reads λ_{t+3} only at the
@@ -461,6 +514,7 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       A.lam2 = lam[i2];
       A.lam3 = lam[i3];
       A.lamn = ln;
+      A.G = G[gi];
       for (int a = 0; a < p->ndim; ++a)
         for (int sd = 0; sd < 2; ++sd) {
           A.nu_old[a][sd] = nu[a][sd][par];
@@ -473,14 +527,23 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       const T* pm1 = want_grad ? seg[t - s] : nullptr;
       const T* p0 = want_grad ? seg[t - s + 1] : nullptr;
       const T* pp1 = want_grad ? seg[t - s + 2] : nullptr;
-      awc::adj_nu_grad<T><<<grid, blk, 0, st>>>(A, pm1, p0, pp1, grad);
+      awc::adj_grad<T><<<grid, blk, 0, st>>>(A, G[gi ^ 1], pm1, p0, pp1, grad);
       if (nsrc > 0)
         awc::adj_sources<T><<<1, 32, 0, st>>>(ln, A.F, snode_d, (int32_t)nsrc, stf_d + t * nsrc,
                                               grad, sout_d ? sout_d + t * nsrc : nullptr);
-      awc::adj_mu<T><<<grid, blk, 0, st>>>(A);
+      for (int a = 0; a < p->ndim; ++a)
+        for (int sd = 0; sd < 2; ++sd) {
+          if (!A.active[a][sd] || h == 0) continue;
+          const int64_t n1 = a == 0 ? p->ny - 2 : p->nx - 2;
+          const int64_t n2 = p->ndim == 3 ? (a == 2 ? p->ny - 2 : V.nz - 2) : 1;
+          const int64_t count = h * n1 * n2;
+          const unsigned nb = (unsigned)std::min<int64_t>((count + 255) / 256, (int64_t)C->num_sms * 8);
+          awc::adj_band<T><<<nb, 256, 0, st>>>(A, a, sd, count);
+        }
       ADJ_TRY(C, cudaGetLastError());
       std::swap(i2, i3);  // λ_{t+1} is the next step's λ_{t+2}
       par ^= 1;
+      gi ^= 1;
     }
   }
   // outputs
@@ -535,26 +598,11 @@ int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
   if (checkpoint_every < 1) return awc::fail(ctx, AWC_ERR_INVALID, "checkpoint_every must be >= 1");
   awc_plan* plan = nullptr;
   if ((rc = awc_plan_create(ctx, p, vel, coeffs, possrcs, dt2srctf, posrecs, &plan))) return rc;
-  // forward traces and residuals
-  const int64_t nt = p->nt, nrec = p->nrec;
-  std::vector<double> tr(std::max<int64_t>(nt * nrec, 1));
-  if ((rc = awc_plan_run(plan, nt, 1, nullptr)) || (nt * nrec > 0 && (rc = awc_plan_traces(plan, tr.data())))) {
-    awc_plan_destroy(plan);
-    return rc;
-  }
-  double J = 0.0;
-  std::vector<double> res(tr.size(), 0.0);
-  for (int64_t c = 0; c < nt * nrec; ++c) {
-    res[c] = tr[c] - observed[c];
-    J += 0.5 * res[c] * res[c];
-  }
-  *misfit = J;
-  if (traces && nt * nrec > 0) std::memcpy(traces, tr.data(), nt * nrec * sizeof(double));
   rc = p->precision == AWC_F64
-           ? adjoint_impl<double>(ctx, plan, p, possrcs, dt2srctf, posrecs, res.data(),
-                                  checkpoint_every, grad_c2, nullptr)
-           : adjoint_impl<float>(ctx, plan, p, possrcs, dt2srctf, posrecs, res.data(),
-                                 checkpoint_every, grad_c2, nullptr);
+           ? adjoint_impl<double>(ctx, plan, p, possrcs, dt2srctf, posrecs, nullptr, observed,
+                                  misfit, traces, checkpoint_every, grad_c2, nullptr)
+           : adjoint_impl<float>(ctx, plan, p, possrcs, dt2srctf, posrecs, nullptr, observed,
+                                 misfit, traces, checkpoint_every, grad_c2, nullptr);
   awc_plan_destroy(plan);
   return rc;
 }
@@ -573,10 +621,10 @@ int awc_adjoint_sources(awc_ctx* ctx, const awc_problem* p, const double* vel,
   std::vector<double> zero(std::max<int64_t>(p->nt * p->nsrc, 1), 0.0);
   if ((rc = awc_plan_create(ctx, p, vel, coeffs, possrcs, zero.data(), posrecs, &plan))) return rc;
   rc = p->precision == AWC_F64
-           ? adjoint_impl<double>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces, 1,
-                                  nullptr, src_out)
-           : adjoint_impl<float>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces, 1,
-                                 nullptr, src_out);
+           ? adjoint_impl<double>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces,
+                                  nullptr, nullptr, nullptr, 1, nullptr, src_out)
+           : adjoint_impl<float>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces,
+                                 nullptr, nullptr, nullptr, 1, nullptr, src_out);
   awc_plan_destroy(plan);
   return rc;
 }

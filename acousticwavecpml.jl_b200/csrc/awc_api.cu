@@ -217,6 +217,11 @@ struct awc_plan {
   int32_t active[3][2] = {};
   std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
   uint64_t graph_key = 0;  // launch configuration the graphs were captured with
+  // copy of each new field to keep: after step it in [keep_first,
+  // keep_first + keep_count) the new field goes to keep[it - keep_first]
+  // (eager runs only; set by the adjoint's segment recompute)
+  void* const* keep = nullptr;
+  int64_t keep_first = 0, keep_count = 0;
 
   int alloc(void** out, size_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -755,6 +760,9 @@ int launch_range(awc_plan* P, int64_t start, int64_t n, cudaStream_t st) {
   for (int64_t it = start; it < start + n; ++it) {
     int rc = P->p.precision == AWC_F64 ? launch_step<double>(P, it, st) : launch_step<float>(P, it, st);
     if (rc) return rc;
+    if (P->keep && it >= P->keep_first && it < P->keep_first + P->keep_count)
+      CUDA_TRY(&P->ctx->err, cudaMemcpyAsync(P->keep[it - P->keep_first], P->buf[(it + 2) % 3],
+                                             P->NP * P->esz, cudaMemcpyDeviceToDevice, st));
   }
   return AWC_OK;
 }
@@ -933,6 +941,12 @@ PlanView plan_view(awc_plan* P) {
 }
 
 void plan_set_step(awc_plan* P, int64_t step) { P->step = step; }
+
+void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count) {
+  P->keep = dst;
+  P->keep_first = first;
+  P->keep_count = dst ? count : 0;
+}
 }  // namespace awc
 
 // ---------------------------------------------------------------------------
@@ -1103,6 +1117,7 @@ int awc_plan_run(awc_plan* P, int64_t nsteps, int32_t use_graph, float* ms) {
   if (n <= 0) return AWC_OK;
   int rc;
   if ((rc = prepare_launch(P))) return rc;
+  if (P->keep) use_graph = 0;  // field copies are made by eager runs only
   cudaGraphExec_t ex = nullptr;
   if (use_graph && (rc = get_graph(P, P->step, n, &ex))) return rc;
   CUDA_TRY(&C->err, cudaEventRecord(C->ev0, C->stream));

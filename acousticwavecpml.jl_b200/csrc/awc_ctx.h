@@ -42,6 +42,9 @@ struct PlanView {
 PlanView plan_view(awc_plan* P);
 // Sets the step counter of a plan whose state was restored from a copy.
 void plan_set_step(awc_plan* P, int64_t step);
+// During eager runs, copies the new field of each step it in [first,
+// first + count) to dst[it - first] (stream-ordered); NULL stops it.
+void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count);
 
 // Sets the calling thread's last error (awc_last_error(NULL)) and, when ctx
 // is not NULL, the context's; returns code.

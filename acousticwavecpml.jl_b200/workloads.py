@@ -116,6 +116,37 @@ def config3(nt=3000, seed=4321, shots_per_model=16, interiors=CONFIG3_INTERIORS,
                 kwargs=dict(halo=halo, rcoef=1e-4, freetop=True, nt=nt))
 
 
+def config4(nt=1500, seed=77, interior=(192, 192, 192), halo=20, dx=10.0):
+    """3D gradient workload: 192^3 interior (232 x 212 x 232 nodes, depth on
+    the second axis, free top), dx = 10 m, c = 2000 + depth_m for the initial
+    model; the true model adds a Gaussian blob of +10 % (radius 20 nodes,
+    seeded centre in the interior). 16 Ricker shots (f0 = 8 Hz, t0 = 1.2 / f0)
+    on a 4 x 4 grid at depth node j = 3, 48 x 48 receivers at j = 3 over the
+    interior, nt common, dt = 0.6 dx / (cmax sqrt 3) of the true model,
+    checkpoint every 50 steps."""
+    ix, iy, iz = interior
+    nx, ny, nz = ix + 2 * halo, iy + halo, iz + 2 * halo
+    depth = np.arange(ny, dtype=np.float64) * dx
+    init = np.asfortranarray(np.broadcast_to((2000.0 + depth)[None, :, None], (nx, ny, nz)))
+    rng = np.random.default_rng(seed)
+    cx, cy, cz = (int(rng.integers(halo + 40, halo + n - 40)) for n in (ix, iy, iz))
+    cy -= halo  # depth axis has no top band
+    X, Y, Z = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    blob = np.exp(-((X - cx) ** 2 + (Y - cy) ** 2 + (Z - cz) ** 2) / (2 * 20.0 ** 2))
+    true = np.asfortranarray(init * (1.0 + 0.10 * blob))
+    dt = 0.6 * dx / (float(true.max()) * math.sqrt(3.0))
+    f0 = 8.0
+    xs = [halo + 1 + round((a + 0.5) * (ix - 1) / 4) for a in range(4)]
+    shots = [[[(i - 1) * dx, 2 * dx, (k - 1) * dx]] for k in xs for i in xs]
+    ridx = [halo + 1 + round(a * (ix - 1) / 47) for a in range(48)]
+    recs = [[(i - 1) * dx, 2 * dx, (k - 1) * dx] for k in ridx for i in ridx]
+    L = ((nx - 1) * dx, (ny - 1) * dx, (nz - 1) * dx)
+    return dict(name=f"cpml3d_grad_{nx}x{ny}x{nz}_16shots_nt{nt}", lengths=L, true=true,
+                init=init, shots=shots, t0s=[1.2 / f0], f0=f0, rec_pos=recs,
+                kwargs=dict(halo=halo, rcoef=1e-4, freetop=True, dt=dt, nt=nt),
+                checkpoint_every=50)
+
+
 def batch_shots(pkg, w):
     """(model index, Sources, Receivers) per shot of a batched workload."""
     out = []
