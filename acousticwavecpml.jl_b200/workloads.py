@@ -119,8 +119,8 @@ def config3(nt=3000, seed=4321, shots_per_model=16, interiors=CONFIG3_INTERIORS,
 def config4(nt=1500, seed=77, interior=(192, 192, 192), halo=20, dx=10.0):
     """3D gradient workload: 192^3 interior (232 x 212 x 232 nodes, depth on
     the second axis, free top), dx = 10 m, c = 2000 + depth_m for the initial
-    model; the true model adds a Gaussian blob of +10 % (radius 20 nodes,
-    seeded centre in the interior). 16 Ricker shots (f0 = 8 Hz, t0 = 1.2 / f0)
+    model; the true model adds a blob of +10 % at its centre, (1 - r²/R²)²
+    with R = 20 nodes and zero beyond (seeded centre in the interior). 16 Ricker shots (f0 = 8 Hz, t0 = 1.2 / f0)
     on a 4 x 4 grid at depth node j = 3, 48 x 48 receivers at j = 3 over the
     interior, nt common, dt = 0.6 dx / (cmax sqrt 3) of the true model,
     checkpoint every 50 steps."""
@@ -129,10 +129,12 @@ def config4(nt=1500, seed=77, interior=(192, 192, 192), halo=20, dx=10.0):
     depth = np.arange(ny, dtype=np.float64) * dx
     init = np.asfortranarray(np.broadcast_to((2000.0 + depth)[None, :, None], (nx, ny, nz)))
     rng = np.random.default_rng(seed)
-    cx, cy, cz = (int(rng.integers(halo + 40, halo + n - 40)) for n in (ix, iy, iz))
+    cx, cy, cz = (int(rng.integers(halo + min(40, n // 4), halo + n - min(40, n // 4)))
+                  for n in (ix, iy, iz))
     cy -= halo  # depth axis has no top band
     X, Y, Z = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
-    blob = np.exp(-((X - cx) ** 2 + (Y - cy) ** 2 + (Z - cz) ** 2) / (2 * 20.0 ** 2))
+    r2 = ((X - cx) ** 2 + (Y - cy) ** 2 + (Z - cz) ** 2) / 20.0 ** 2
+    blob = np.where(r2 < 1.0, (1.0 - r2) ** 2, 0.0)  # smooth, zero beyond 20 nodes
     true = np.asfortranarray(init * (1.0 + 0.10 * blob))
     dt = 0.6 * dx / (float(true.max()) * math.sqrt(3.0))
     f0 = 8.0

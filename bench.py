@@ -260,6 +260,62 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak):
             "sharding": f"shots {rank}::{world} per rank" if world > 1 else "one batch"}
 
 
+def gradient_leg(pkg, ctx, rank, world, timed_host):
+    """3D gradient, FP32 with an FP64 check: one shot of the 16-shot
+    gradient workload per rank (shot = rank), dJ/d(c²) at the initial model
+    against the true model's traces of the same precision, through
+    awc_misfit_gradient (host
+    buffers, checkpoint every 50 steps, nt = 1500); under torchrun the ranks'
+    gradients are then summed with one all-reduce."""
+    import time
+    import torch
+    import torch.distributed as dist
+    from acousticwavecpml_b200 import adjoint
+    from acousticwavecpml_b200 import workloads as W
+    w = W.config4()
+    S = pkg.Sources(w["shots"][rank % len(w["shots"])], w["t0s"], [pkg.rickersource1D], w["f0"])
+    R = pkg.Receivers(w["rec_pos"])
+    kw = dict(w["kwargs"])
+    st = pkg.prepare(w["lengths"], None, w["true"], S, R, precision="f32", **kw)
+    p = st["problem"]
+    obs = np.zeros((p.nt, p.nrec), order="F")
+    ctx.forward(p, st["vel"], st["coeffs"], st["possrcs"], st["dt2srctf"], st["posrecs"], obs)
+    t0 = time.perf_counter()
+    ctx.forward(p, st["vel"], st["coeffs"], st["possrcs"], st["dt2srctf"], st["posrecs"], obs)
+    t_fwd = time.perf_counter() - t0
+    si = pkg.prepare(w["lengths"], None, w["init"], S, R, precision="f32", **kw)
+    si["coeffs"] = st["coeffs"]  # the CPML profile of the true model's vmax
+    adjoint.misfit_gradient(si, obs, w["checkpoint_every"], ctx)  # warm-up
+    t_grad = timed_host(lambda: adjoint.misfit_gradient(si, obs, w["checkpoint_every"], ctx))
+    J32, g32, _ = adjoint.misfit_gradient(si, obs, w["checkpoint_every"], ctx)
+    # the FP64 build on FP64 data of the true model
+    s64t = pkg.prepare(w["lengths"], None, w["true"], S, R, precision="f64", **kw)
+    obs64 = np.zeros((p.nt, p.nrec), order="F")
+    ctx.forward(s64t["problem"], s64t["vel"], s64t["coeffs"], s64t["possrcs"], s64t["dt2srctf"],
+                s64t["posrecs"], obs64)
+    s64 = pkg.prepare(w["lengths"], None, w["init"], S, R, precision="f64", **kw)
+    s64["coeffs"] = st["coeffs"]
+    J64, g64, _ = adjoint.misfit_gradient(s64, obs64, w["checkpoint_every"], ctx)
+    t_ar = 0.0
+    if world > 1:
+        buf = torch.from_numpy(np.ascontiguousarray(g32.ravel(order="F"))).cuda()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dist.all_reduce(buf)
+        torch.cuda.synchronize()
+        t_ar = time.perf_counter() - t0
+    return {"workload": w["name"], "dtype": "f32", "shots_per_rank": 1,
+            "value": world / t_grad, "unit": "shot gradients/s",
+            "s_per_gradient": t_grad, "s_per_forward": t_fwd,
+            "gradient_over_forward": t_grad / t_fwd, "checkpoint_every": w["checkpoint_every"],
+            "nt": p.nt, "grid": [p.nx, p.ny, p.nz],
+            "fp32_vs_fp64_gradient_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+            "fp32_vs_fp64_misfit_rel": abs(J32 - J64) / J64,
+            "allreduce_s": t_ar,
+            "timing": "host wall clock of the C-ABI call (uploads, checkpointed forward, "
+                      "recompute, adjoint, download), max over ranks"}
+
+
 def main():
     args = parse_args()
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -411,6 +467,22 @@ def main():
 
         # ---- batched 2D shots (96 shots over 6 layered models), sharded -----
         line["batch"] = batch_leg(pkg, ctx, args, rank, world, timed, peak)
+
+        # ---- 3D gradient by the discrete adjoint (one shot per rank) -------
+        def timed_host(fn):
+            import time
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            fn()
+            t = time.perf_counter() - t0
+            if world > 1:
+                tt = torch.tensor([t], device="cuda")
+                dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+                t = float(tt.item())
+            return t
+
+        line["gradient"] = gradient_leg(pkg, ctx, rank, world, timed_host)
 
         # ---- CPU baseline (rank 0 at N=1 only) ------------------------------
         if world == 1 and rank == 0:
