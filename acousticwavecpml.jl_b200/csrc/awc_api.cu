@@ -156,10 +156,12 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// Pipeline depth of the 3D step kernel: S stages let the TMA loads run S-3
-// planes ahead of the plane being computed.
+// Pipeline depth of the 3D core kernel: S stages let the TMA loads run S-3
+// planes ahead of the plane being computed. Four stages (one plane ahead)
+// keep the blocks small, so that more of them, and of the band kernel's,
+// share an SM; that measured faster than 5, 6 or 8 stages.
 template <typename T>
-constexpr int stages() { return sizeof(T) == 4 ? 6 : 4; }
+constexpr int stages() { return 4; }
 
 }  // namespace
 
