@@ -112,6 +112,8 @@ SIGNATURES = {
     "awc_misfit_gradient": (ctypes.c_int, [_vp, _PP, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int32,
                                            _vp, _vp, _vp]),
     "awc_adjoint_sources": (ctypes.c_int, [_vp, _PP, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "awc_learned_weights_len": (ctypes.c_int, [ctypes.c_int32]),
+    "awc_forward_learned": (ctypes.c_int, [_vp, _PP, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "awc_forward2d_f32_static": (ctypes.c_int, [_PP, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "awc_batch_create": (ctypes.c_int, [_vp, ctypes.c_int32, _PP, _vp, ctypes.c_int32, _vp,
                                         ctypes.POINTER(_vp)]),

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["csrc/awc_api.cu", "csrc/awc_adjoint.cu", "csrc/awc_batch.cu", "csrc/awc_static.cu"]
+SOURCES = ["csrc/awc_api.cu", "csrc/awc_adjoint.cu", "csrc/awc_batch.cu", "csrc/awc_learned.cu", "csrc/awc_static.cu"]
 HEADERS = ["csrc/awc_kernels.cuh", "csrc/awc_ctx.h", "../include/awcpml.h"]
 OUT = os.path.join(HERE, "lib", "libawcpml.so")
 

@@ -230,6 +230,23 @@ int awc_adjoint_sources(awc_ctx* ctx, const awc_problem* p, const double* vel,
                         const double* coeffs, const int64_t* possrcs, const int64_t* posrecs,
                         const double* adjoint_traces, double* src_out);
 
+/* ---- Learned thin absorbing layer --------------------------------------------
+ * No counterpart in the reference. awc_forward with the CPML replaced by a
+ * layer of p->halo (1..8) nodes on every absorbing side whose new values come
+ * from a small MLP: the block of 3^d nodes around a layer node at the three
+ * latest time levels (K = 27 in 2D, 81 in 3D inputs, oriented along the
+ * nearest side's outward normal and scaled by their largest magnitude), then
+ * K -> 32 -> 32 -> 1 with ReLU. Interior nodes take the plain leapfrog step.
+ * FP32 only (p->precision == AWC_F32); `coeffs` are not used; sources and
+ * receivers must be interior nodes. weights_bf16: awc_learned_weights_len(ndim)
+ * BF16 values, W1 (32 x K, row-major), b1 (32), W2 (32 x 32), b2 (32),
+ * W3 (32), b3 (1). */
+int awc_learned_weights_len(int32_t ndim);
+int awc_forward_learned(awc_ctx* ctx, const awc_problem* p, const double* vel,
+                        const uint16_t* weights_bf16, const int64_t* possrcs,
+                        const double* dt2srctf, const int64_t* posrecs, double* traces,
+                        double* pfinal);
+
 /* awc_forward for 2D FP32 problems without any device memory allocation.
  * No counterpart in the reference (its solvers always allocate).
  *
