@@ -9,7 +9,9 @@
 //       along the outward normal u = -1, 0, +1 of the nearest absorbing side,
 //       then along the remaining axes in increasing axis order;
 //   s = max |x| (or 1 when x = 0), so that the layer is linear in amplitude;
-//   MLP: K -> 32 -> 32 -> 1 with ReLU, K = 3 * 3^d (27 in 2D, 81 in 3D),
+//   MLP: K -> 32 -> 32 -> 1 with ReLU over x / s and the local Courant number
+//       r = c dt / d along the normal (K = 3 * 3^d + 1: 28 in 2D, 82 in 3D;
+//       without r a local operator cannot tell how fast the wave leaves),
 //       weights in BF16, products accumulated in FP32.
 // A node within W of two sides uses the nearer one (x before y before z on
 // ties). Sources are added after the update, then receivers sample p_{t+1}.
@@ -27,12 +29,13 @@
 namespace {
 
 constexpr int kHid = 32;
-constexpr int kMaxIn = 81;
+constexpr int kMaxIn = 82;
 
 struct LearnedParams {
   int32_t ndim, nx, ny, nz, width, freetop;
   int64_t px, plane;
   float inv_d2[3];
+  float inv_d[3];
   const float* F;
   const float* p0;  // p_{t-2}
   const float* p1;  // p_{t-1}
@@ -132,11 +135,13 @@ __global__ void __launch_bounds__(256) learned_layer(LearnedParams L) {
           s = fmaxf(s, fabsf(val));
         }
   const float inv = s > 0.f ? 1.f / s : 1.f;
+  for (int c = 0; c < f; ++c) x[c] *= inv;
+  x[f] = sqrtf(L.F[i + L.px * j + L.plane * k]) * L.inv_d[ax];  // Courant number
   float h1[kHid];
 #pragma unroll 4
   for (int r = 0; r < kHid; ++r) {
     float acc = b1[r];
-    for (int c = 0; c < K; ++c) acc = fmaf(W1[r * K + c], x[c] * inv, acc);
+    for (int c = 0; c < K; ++c) acc = fmaf(W1[r * K + c], x[c], acc);
     h1[r] = fmaxf(acc, 0.f);
   }
   float out = b3;
@@ -204,7 +209,7 @@ extern "C" {
 
 int awc_learned_weights_len(int32_t ndim) {
   if (ndim != 2 && ndim != 3) return 0;
-  const int K = ndim == 3 ? 81 : 27;
+  const int K = ndim == 3 ? 82 : 28;
   return kHid * K + kHid + kHid * kHid + kHid + kHid + 1;
 }
 
@@ -282,10 +287,13 @@ int awc_forward_learned(awc_ctx* ctx, const awc_problem* p, const double* vel,
   L.px = px;
   L.plane = plane;
   const double d[3] = {p->dx, p->dy, p->ndim == 3 ? p->dz : 1.0};
-  for (int a = 0; a < 3; ++a) L.inv_d2[a] = (float)(1.0 / (d[a] * d[a]));
+  for (int a = 0; a < 3; ++a) {
+    L.inv_d2[a] = (float)(1.0 / (d[a] * d[a]));
+    L.inv_d[a] = (float)(1.0 / d[a]);
+  }
   L.F = F;
   L.w = w_d;
-  L.nin = p->ndim == 3 ? 81 : 27;
+  L.nin = p->ndim == 3 ? 82 : 28;
   const dim3 blk(32, 8);
   const dim3 grid((unsigned)((p->nx - 2 + 31) / 32), (unsigned)((p->ny - 2 + 7) / 8),
                   (unsigned)(p->ndim == 3 ? nz - 2 : 1));

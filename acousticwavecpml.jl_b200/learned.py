@@ -30,7 +30,18 @@ DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 
 
 def n_inputs(ndim):
-    return 27 if ndim == 2 else 81
+    """3 time levels x 3^d nodes, plus the local Courant number."""
+    return 28 if ndim == 2 else 82
+
+
+def courant(vel, dt, d, coords, ax):
+    """c dt / d along each layer node's normal axis (the kernel forms it as
+    sqrt(F) / d with F = dt² c² in FP32)."""
+    ndim = vel.ndim
+    c = vel[tuple(coords[:, a] for a in range(ndim))]
+    dd = np.asarray(d, dtype=np.float64)[ax]
+    F = (dt * dt * c.astype(np.float64) ** 2).astype(np.float32).astype(np.float64)
+    return np.sqrt(F) / dd
 
 
 def weights_len(ndim):
@@ -201,8 +212,9 @@ def reference_fields(pkg, lengths, vel, srcs, recs, *, dt, nt, width, pad=300, h
 
 
 def training_data(pkg, cases, *, width=4, pad=300, every=1, keep=1.0, seed=0, ctx=None):
-    """Inputs and targets (normalised by max |input| per sample) from the
-    reference runs of `cases`: dicts with lengths, vel, srcs, recs, dt, nt,
+    """Inputs (the 3^d block at three levels normalised by its largest
+    magnitude, then the Courant number) and targets (normalised alike) from
+    the reference runs of `cases`: dicts with lengths, vel, srcs, recs, dt, nt,
     freetop. Samples whose inputs are all zero are dropped."""
     rng = np.random.default_rng(seed)
     X, Y = [], []
@@ -213,6 +225,8 @@ def training_data(pkg, cases, *, width=4, pad=300, every=1, keep=1.0, seed=0, ct
         flat_node = coords[:, 0] + shape[0] * coords[:, 1]
         if len(shape) == 3:
             flat_node = flat_node + shape[0] * shape[1] * coords[:, 2]
+        d = [c["lengths"][a] / (shape[a] - 1) for a in range(len(shape))]
+        r = courant(c["vel"], c["dt"], d, coords, ax)
         hist = [np.zeros(shape, order="F")] * 3  # p_{t-2}, p_{t-1}, p_t
         for t, pnew in reference_fields(pkg, c["lengths"], c["vel"], c["srcs"], c["recs"],
                                         dt=c["dt"], nt=c["nt"], width=width, pad=pad,
@@ -224,7 +238,7 @@ def training_data(pkg, cases, *, width=4, pad=300, every=1, keep=1.0, seed=0, ct
                 m = s > 0
                 if keep < 1.0:
                     m &= rng.random(len(m)) < keep
-                X.append((x[m] / s[m, None]).astype(np.float32))
+                X.append(np.concatenate([x[m] / s[m, None], r[m, None]], axis=1).astype(np.float32))
                 Y.append((y[m] / s[m]).astype(np.float32))
             hist = [hist[1], hist[2], pnew]
     return np.concatenate(X), np.concatenate(Y)
@@ -287,6 +301,8 @@ class RolloutSim:
         self.lflat = torch.tensor(coords[:, 0] + nx * coords[:, 1], device=device)
         self.gidx = torch.tensor(np.maximum(gidx, 0), device=device)
         self.gmask = torch.tensor(gidx >= 0, device=device, dtype=torch.float32)
+        self.r = torch.tensor(courant(vel, dt, d, coords, ax), dtype=torch.float32,
+                              device=device)[:, None]
         core = np.zeros((ny, nx), dtype=bool)
         core[1:ny - 1, 1:nx - 1] = True
         lm = np.zeros(nx * ny, dtype=bool)
@@ -305,7 +321,7 @@ class RolloutSim:
         new = (2 * p2 - p1 + self.F * lap) * self.core
         x = torch.cat([f.reshape(-1)[self.gidx] * self.gmask for f in (p0, p1, p2)], dim=1)
         sc = torch.amax(x.abs(), dim=1).clamp_min(1e-30)
-        y = net(x / sc[:, None]).squeeze(1) * sc
+        y = net(torch.cat([x / sc[:, None], self.r], dim=1)).squeeze(1) * sc
         new = new.reshape(-1).index_put((self.lflat,), y, accumulate=True).reshape(p2.shape)
         if t < self.stf.shape[0]:
             new = new.reshape(-1).index_put((torch.tensor([self.src], device=new.device),),
@@ -322,7 +338,7 @@ def train_rollout(net_flat, sims, refs, *, window=100, iters=400, lr=5e-4, seed=
     RolloutSim per case; refs: (nt, ny, nx) reference fields per case."""
     import torch
     rng = np.random.default_rng(seed)
-    k = sims[0].gidx.shape[1] * 3
+    k = sims[0].gidx.shape[1] * 3 + 1
     W1, b1, W2, b2, W3, b3 = unpack(net_flat, 2)
     net = torch.nn.Sequential(torch.nn.Linear(k, HIDDEN), torch.nn.ReLU(),
                               torch.nn.Linear(HIDDEN, HIDDEN), torch.nn.ReLU(),

@@ -234,9 +234,9 @@ int awc_adjoint_sources(awc_ctx* ctx, const awc_problem* p, const double* vel,
  * No counterpart in the reference. awc_forward with the CPML replaced by a
  * layer of p->halo (1..8) nodes on every absorbing side whose new values come
  * from a small MLP: the block of 3^d nodes around a layer node at the three
- * latest time levels (K = 27 in 2D, 81 in 3D inputs, oriented along the
- * nearest side's outward normal and scaled by their largest magnitude), then
- * K -> 32 -> 32 -> 1 with ReLU. Interior nodes take the plain leapfrog step.
+ * latest time levels (oriented along the nearest side's outward normal and
+ * scaled by their largest magnitude) and the local Courant number, K = 28
+ * inputs in 2D, 82 in 3D, then K -> 32 -> 32 -> 1 with ReLU. Interior nodes take the plain leapfrog step.
  * FP32 only (p->precision == AWC_F32); `coeffs` are not used; sources and
  * receivers must be interior nodes. weights_bf16: awc_learned_weights_len(ndim)
  * BF16 values, W1 (32 x K, row-major), b1 (32), W2 (32 x 32), b2 (32),

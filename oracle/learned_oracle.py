@@ -9,7 +9,8 @@ nodes (within `width` of an absorbing side): p_{t+1} = s MLP(x / s), x the
 3^d block around the node at levels t-2, t-1, t (0 outside the interior),
 ordered by level, then along the nearest side's outward normal (-1, 0, +1),
 then along the remaining axes in increasing order; s = max |x| (1 when 0).
-MLP: K -> 32 -> 32 -> 1 with ReLU. Sources are added after the update, then
+MLP: K -> 32 -> 32 -> 1 with ReLU over (x / s, r), r = sqrt(F) / d along
+the normal (the local Courant number), K = 3 * 3^d + 1. Sources are added after the update, then
 receivers sample p_{t+1}.
 """
 import numpy as np
@@ -79,10 +80,11 @@ def forward(vel, d, dt, nt, width, freetop, weights, src_nodes, stf, rec_nodes):
             lap[inner] += (p2[tuple(sl_p)] - 2.0 * p2[inner] + p2[tuple(sl_m)]) / (d[a] * d[a])
         upd = 2.0 * p2 - p1 + F * lap
         new[inner] = upd[inner]
-        for (c, _, _), blk in zip(layer, blocks):
+        for (c, ax, _), blk in zip(layer, blocks):
             x = np.array([lv[q] if q is not None else 0.0 for lv in (p0, p1, p2) for q in blk])
             s = np.abs(x).max()
             xs = x / s if s > 0 else x
+            xs = np.append(xs, np.sqrt(np.float32(F[c])) / d[ax])
             h1 = np.maximum(W1 @ xs + b1, 0.0)
             h2 = np.maximum(W2 @ h1 + b2, 0.0)
             y = float(W3 @ h2 + b3)
