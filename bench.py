@@ -178,6 +178,23 @@ def a_eff(pkg, problem):
     return a_eff_words(problem) * word_bytes(problem)
 
 
+def min_traffic(p):
+    """Bytes per 3D time step a perfect kernel must move: 4 words per interior
+    node (read pold, pcur, fact; write pnew) plus, per active CPML side, one
+    read and one write of every ψ (h+1 layers) and ξ (h layers) entry. The
+    free top leaves one y side inactive."""
+    from acousticwavecpml_b200.core import word_bytes
+    w = word_bytes(p)
+    active_sides = (2, 1 if p.freetop else 2, 2)
+    n = [p.nx - 2, p.ny - 2, p.nz - 2]
+    cells = n[0] * n[1] * n[2]
+    band = 0
+    for a in range(3):
+        cross = cells // n[a]
+        band += active_sides[a] * 2 * ((p.halo + 1) + p.halo) * cross
+    return w * (4 * cells + band)
+
+
 def interior_cells(p):
     return (p.nx - 2) * (p.ny - 2) * ((p.nz - 2) if p.ndim == 3 else 1)
 
@@ -404,6 +421,8 @@ def main():
         "gcells_per_s": world * interior_cells(p) / t_ts / 1e9,
         "us_per_timestep": t_ts * 1e6,
         "a_eff_bytes_per_timestep": ab,
+        "min_traffic_bytes_per_timestep": min_traffic(p),
+        "a_eff_over_min_traffic": ab / min_traffic(p),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src,
