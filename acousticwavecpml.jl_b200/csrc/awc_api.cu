@@ -172,6 +172,7 @@ struct awc_plan {
   int64_t N = 0;   // nodes (dense count)
   int64_t px = 0;  // field row pitch (elements)
   int64_t NP = 0;  // pitched field length
+  int64_t psi_side[3] = {}, xi_side[3] = {};  // right side's ψ / ξ offset from the left's (elements)
   // device buffers
   void* buf[3] = {nullptr, nullptr, nullptr};
   void* fact = nullptr;
@@ -263,6 +264,10 @@ int64_t cross_section(const awc_problem* p, int axis) {
   return axis == 0 ? p->ny * nz : axis == 1 ? px * nz : px * p->ny;
 }
 
+// Elements from the left side's ψ or ξ array of an axis to the right side's:
+// the left array's length rounded up to 64 elements (256-byte aligned starts).
+int64_t side_stride(int64_t len) { return (len + 63) / 64 * 64; }
+
 // Allocates every device buffer of a plan (shape only, contents undefined).
 int plan_alloc(awc_plan* P) {
   const awc_problem* p = &P->p;
@@ -276,13 +281,24 @@ int plan_alloc(awc_plan* P) {
   for (int b = 0; b < 3; ++b)
     if ((rc = P->alloc(&P->buf[b], P->NP * P->esz))) return rc;
   if ((rc = P->alloc(&P->fact, P->NP * P->esz))) return rc;
-  for (int a = 0; a < p->ndim; ++a)
-    for (int s = 0; s < 2; ++s) {
-      const int64_t cs = cross_section(p, a);
-      for (int par = 0; par < 2; ++par)
-        if ((rc = P->alloc(&P->psi[a][s][par], (h + 1) * cs * P->esz))) return rc;
-      if ((rc = P->alloc(&P->xi[a][s], h * cs * P->esz))) return rc;
+  // ψ (each parity) and ξ of an axis: one allocation per array kind, the
+  // right side's array at a fixed offset after the left side's (the 3D band
+  // kernel addresses both sides from the left base)
+  for (int a = 0; a < p->ndim; ++a) {
+    const int64_t cs = cross_section(p, a);
+    P->psi_side[a] = side_stride((h + 1) * cs);
+    P->xi_side[a] = side_stride(h * cs);
+    for (int par = 0; par < 2; ++par) {
+      void* base = nullptr;
+      if ((rc = P->alloc(&base, 2 * P->psi_side[a] * P->esz))) return rc;
+      P->psi[a][0][par] = base;
+      P->psi[a][1][par] = (char*)base + P->psi_side[a] * P->esz;
     }
+    void* base = nullptr;
+    if ((rc = P->alloc(&base, 2 * P->xi_side[a] * P->esz))) return rc;
+    P->xi[a][0] = base;
+    P->xi[a][1] = (char*)base + P->xi_side[a] * P->esz;
+  }
   if ((rc = P->alloc(&P->coef, awc_coeffs_len(p) * P->esz))) return rc;
   if ((rc = P->alloc((void**)&P->err_flag, 4))) return rc;
   const int64_t ns = std::max<int64_t>(p->nsrc, 1), nr = std::max<int64_t>(p->nrec, 1);
@@ -483,6 +499,15 @@ awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
   for (int b2 = 0; b2 < 6; ++b2) S.box[b2] = P->box[b2];
   for (int b2 = 0; b2 < 7; ++b2) S.box_blk[b2] = P->box_blk[b2];
   S.shell_zchunk = P->szc;
+  S.plane = P->px * p->ny;
+  S.psi_dz[0] = (h + 1) * p->ny;
+  S.xi_dz[0] = h * p->ny;
+  S.psi_dz[1] = P->px * (h + 1);
+  S.xi_dz[1] = P->px * h;
+  for (int a = 0; a < 3; ++a) {
+    S.psi_side[a] = P->psi_side[a];
+    S.xi_side[a] = P->xi_side[a];
+  }
   return S;
 }
 
@@ -511,38 +536,44 @@ void make_regions(awc_plan* P) {
     empty = empty || lo[a] > hi[a];
   }
   P->nbox = 0;
-  auto add = [&](int64_t x0, int64_t x1, int64_t y0, int64_t y1, int64_t z0, int64_t z1) {
+  // kind: 7 z slab, 3 y slab, 1 x slab, 15 no core (the band kernel's body)
+  auto add = [&](int64_t x0, int64_t x1, int64_t y0, int64_t y1, int64_t z0, int64_t z1,
+                 int32_t kind) {
     if (x0 > x1 || y0 > y1 || z0 > z1) return;
     P->box[P->nbox++] = awc::Box{(int32_t)x0, (int32_t)x1, (int32_t)y0, (int32_t)y1,
-                                 (int32_t)z0, (int32_t)z1};
+                                 (int32_t)z0, (int32_t)z1, kind};
   };
   if (empty) {
     P->has_core = false;
-    add(1, n[0] - 2, 1, n[1] - 2, 1, n[2] - 2);
+    add(1, n[0] - 2, 1, n[1] - 2, 1, n[2] - 2, 15);
   } else {
     P->has_core = true;
     P->core = awc::Box{(int32_t)lo[0], (int32_t)hi[0], (int32_t)lo[1], (int32_t)hi[1],
-                       (int32_t)lo[2], (int32_t)hi[2]};
+                       (int32_t)lo[2], (int32_t)hi[2], 0};
     const int64_t align = 16 / (int64_t)P->esz;  // TMA x origin alignment
     P->core_x = (int32_t)(lo[0] / align * align);
-    add(1, n[0] - 2, 1, n[1] - 2, 1, lo[2] - 1);
-    add(1, n[0] - 2, 1, n[1] - 2, hi[2] + 1, n[2] - 2);
-    add(1, n[0] - 2, 1, lo[1] - 1, lo[2], hi[2]);
-    add(1, n[0] - 2, hi[1] + 1, n[1] - 2, lo[2], hi[2]);
-    add(1, lo[0] - 1, lo[1], hi[1], lo[2], hi[2]);
-    add(hi[0] + 1, n[0] - 2, lo[1], hi[1], lo[2], hi[2]);
+    add(1, n[0] - 2, 1, n[1] - 2, 1, lo[2] - 1, 7);
+    add(1, n[0] - 2, 1, n[1] - 2, hi[2] + 1, n[2] - 2, 7);
+    add(1, n[0] - 2, 1, lo[1] - 1, lo[2], hi[2], 3);
+    add(1, n[0] - 2, hi[1] + 1, n[1] - 2, lo[2], hi[2], 3);
+    add(1, lo[0] - 1, lo[1], hi[1], lo[2], hi[2], 1);
+    add(hi[0] + 1, n[0] - 2, lo[1], hi[1], lo[2], hi[2], 1);
   }
   box_blocks(P);
 }
 
-// Block ranges of the band kernel: box b has 32 x 8 column tiles times
-// chunks of szc planes.
+// Block ranges of the band kernel: box b has its W x H columns in runs of
+// BAND_NT times chunks of szc planes.
+int64_t band_col_blocks(const awc::Box& B) {
+  const int64_t ncol = (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
+  return (ncol + awc::BAND_NT - 1) / awc::BAND_NT;
+}
+
 void box_blocks(awc_plan* P) {
   P->box_blk[0] = 0;
   for (int b = 0; b < P->nbox; ++b) {
     const awc::Box& B = P->box[b];
-    const int64_t blocks = (int64_t)((B.x1 - B.x0 + 32) / 32) * ((B.y1 - B.y0 + 8) / 8) *
-                           ((B.z1 - B.z0 + P->szc) / P->szc);
+    const int64_t blocks = band_col_blocks(B) * ((B.z1 - B.z0 + P->szc) / P->szc);
     P->box_blk[b + 1] = (int32_t)(P->box_blk[b] + blocks);
   }
   for (int b = P->nbox; b < 6; ++b) P->box_blk[b + 1] = P->box_blk[b];
@@ -606,10 +637,10 @@ int ensure_io(awc_plan* P) {
     for (int b = 0; b < P->nbox; ++b) {
       const awc::Box& B = P->box[b];
       if (i < B.x0 || i > B.x1 || j < B.y0 || j > B.y1 || k < B.z0 || k > B.z1) continue;
-      const int64_t gx = (B.x1 - B.x0 + 32) / 32, gy = (B.y1 - B.y0 + 8) / 8;
-      const int64_t blk = P->box_blk[b] + (i - B.x0) / 32 +
-                          gx * ((j - B.y0) / 8 + gy * ((k - B.z0) / P->szc));
-      const int local = (int)((i - B.x0) % 32 + 32 * ((j - B.y0) % 8));
+      const int64_t l = (i - B.x0) + (int64_t)(B.x1 - B.x0 + 1) * (j - B.y0);
+      const int64_t blk = P->box_blk[b] + l / awc::BAND_NT +
+                          band_col_blocks(B) * ((k - B.z0) / P->szc);
+      const int local = (int)(l % awc::BAND_NT);
       ent[1].push_back({{blk, (k << 32) | local}, make_int4(local, (int)k, e.sgrp, e.rgrp)});
       break;
     }
@@ -734,8 +765,13 @@ int launch_step(awc_plan* P, int64_t it, cudaStream_t st) {
     if (shell) {
       awc::StepParams<T> Sh = S;
       kernel_params(P, 1, Sh);
-      awc::step3d_band<T><<<(unsigned)P->box_blk[P->nbox], dim3(32, 8), 0,
-                             core ? C->stream2 : st>>>(Sh);
+      cudaStream_t sb = core ? C->stream2 : st;
+      // offsets fit in int32 when every field (and so every ψ/ξ array) does
+      const unsigned nb = (unsigned)P->box_blk[P->nbox];
+      if (P->NP <= (int64_t)INT32_MAX)
+        awc::step3d_band<T, int32_t><<<nb, awc::BAND_NT, 0, sb>>>(Sh);
+      else
+        awc::step3d_band<T, int64_t><<<nb, awc::BAND_NT, 0, sb>>>(Sh);
     }
     if (core) {
       kernel_params(P, 0, S);

@@ -79,6 +79,7 @@ struct Io {
 // Inclusive 0-based node ranges of an axis-aligned box.
 struct Box {
   int32_t x0, x1, y0, y1, z0, z1;
+  int32_t kind;  // band kernel: which bands the box's nodes lie in (1, 3, 7 or 15)
 };
 
 template <typename T>
@@ -109,6 +110,9 @@ struct StepParams {
   Box box[6];
   int32_t box_blk[7];
   int32_t shell_zchunk;  // planes per block of the band kernel
+  int64_t plane;             // px * ny
+  int64_t psi_dz[2], xi_dz[2];  // x and y: ψ / ξ element step from one z plane to the next
+  int64_t psi_side[3], xi_side[3];  // element offset of the right side's ψ / ξ from the left's
 };
 
 // Node arithmetic with its rounding pinned. Every kernel forms a second
@@ -148,15 +152,26 @@ __device__ __forceinline__ BandCoef<T> band_coef(const BandSide<T>& B, int q) {
 // ψ[q] = b/K_half[q] ψ[q] + a_half[q] (pp - pc) / d, ψ[q-1] likewise with
 // (pc - pm); dψ = (ψ[q] - ψ[q-1]) / d; ξ = b/K[q-1] ξ + a[q-1] (d2 + dψ);
 // damp += f (dψ + ξ).
+// psi_face: the new ψ on one face from its old value and the pressure jump
+// dp across it; cpml_tail: dψ, ξ and the damping term from both faces' ψ.
+template <typename T>
+__device__ __forceinline__ T psi_face(T bh, T ah, T ps, T dp, T inv) {
+  return fma(bh, ps, mul_rn(mul_rn(ah, dp), inv));
+}
+template <typename T>
+__device__ __forceinline__ void cpml_tail(T bk, T a, T sq, T sm, T xo, T d2, T f, T inv, T& xn,
+                                          T& damp) {
+  const T dps = mul_rn(sq - sm, inv);
+  xn = fma(bk, xo, mul_rn(a, d2 + dps));
+  damp = fma(f, dps + xn, damp);
+}
 template <typename T>
 __device__ __forceinline__ void cpml_axis(const BandCoef<T>& c, T psq, T psm, T xo, T pm, T pc,
                                           T pp, T d2, T f, T inv, T& sq, T& sm, T& xn,
                                           T& damp) {
-  sq = fma(c.bh, psq, mul_rn(mul_rn(c.ah, pp - pc), inv));
-  sm = fma(c.bhm, psm, mul_rn(mul_rn(c.ahm, pc - pm), inv));
-  const T dps = mul_rn(sq - sm, inv);
-  xn = fma(c.bk, xo, mul_rn(c.a, d2 + dps));
-  damp = fma(f, dps + xn, damp);
+  sq = psi_face(c.bh, c.ah, psq, pp - pc, inv);
+  sm = psi_face(c.bhm, c.ahm, psm, pc - pm, inv);
+  cpml_tail(c.bk, c.a, sq, sm, xo, d2, f, inv, xn, damp);
 }
 
 // Which band (if any) coordinate c of an axis of length n lies in.
@@ -452,13 +467,14 @@ __global__ void __launch_bounds__(32 * TY) step3d_core(const __grid_constant__ C
 }
 
 // CPML update of one band axis at one node whose ψ entry q sits at element
-// `pq` of the side's arrays (ψ[q-1] at pq - dq) and ξ entry q-1 at `xq`.
-template <typename T>
-__device__ __forceinline__ void band_apply(const BandSide<T>& B, int q, bool first, int64_t pq,
-                                           int64_t dq, int64_t xq, T psq, T psm, T xo, T pm,
-                                           T pc, T pp, T d2, T f, T inv, T& damp) {
+// `pq` of the side's arrays (ψ[q-1] at pq - dq) and ξ entry q-1 at `xq`;
+// c holds the entry's coefficients.
+template <typename T, typename I>
+__device__ __forceinline__ void band_apply(const BandSide<T>& B, const BandCoef<T>& c, bool first,
+                                           I pq, I dq, I xq, T psq, T psm, T xo, T pm, T pc,
+                                           T pp, T d2, T f, T inv, T& damp) {
   T sq, sm, xn;
-  cpml_axis(band_coef(B, q), psq, psm, xo, pm, pc, pp, d2, f, inv, sq, sm, xn, damp);
+  cpml_axis(c, psq, psm, xo, pm, pc, pp, d2, f, inv, sq, sm, xn, damp);
   B.psi_new[pq] = sq;
   if (first) B.psi_new[pq - dq] = sm;
   B.xi[xq] = xn;
@@ -466,117 +482,236 @@ __device__ __forceinline__ void band_apply(const BandSide<T>& B, int q, bool fir
 
 // ---------------------------------------------------------------------------
 // 3D band step: the interior nodes outside P.core (the CPML bands), in the
-// boxes P.box[0..nbox). A block of 32 x 8 threads owns a 32 x 8 column tile
-// of a box and streams `zchunk`-plane chunks of it (P.shell_zchunk); each
-// thread keeps its column's z neighbours in registers, and its x and y band
-// state (entry pointers and coefficients, fixed along z) in registers. The
-// z band, uniform over a plane, is looked up per plane.
+// boxes P.box[0..nbox). The (x, y) columns of a box are numbered row by row,
+// l = (i - x0) + W (j - y0) with W the box width, so the 20-node-wide x slabs
+// waste no thread slots; a block of BAND_NT threads owns BAND_NT consecutive
+// columns and streams a chunk of P.shell_zchunk planes of them, keeping each
+// column's z neighbours in registers.
+//
+// Box.kind says which bands the nodes of a box lie in, and the block body is
+// compiled per kind:
+//   1  an x slab: every node lies in the x band of the slab's side;
+//   3  a y slab: every node lies in the y band of the slab's side, the
+//      columns at its x ends in an x band too;
+//   7  a z slab: every node lies in the z band of the slab's side, the
+//      columns at its x and y edges in x and y bands too;
+//   15 a grid without a core: any band anywhere.
+// The right side's ψ, ξ and coefficient arrays of an axis follow the left
+// side's at fixed offsets (P.psi_side, P.xi_side; halo + 1 and halo
+// coefficients), so every band access is the left side's base pointer plus
+// an offset with the side folded in, and no pointer is selected per thread.
+// x and y entries are fixed along a column (offsets and, in their own slab,
+// coefficients held in registers); in a z slab ψ[q] of node (i, j, k) sits at
+// the node's own field offset less a constant. Integer offsets are of type
+// I: int32 when every field fits, else int64. Along z the new ψ on a node's
+// lower face is the value the column computed on the previous plane's upper
+// face (the same operations on the same operands), so it is carried instead
+// of recomputed.
+constexpr int BAND_NT = 256;
+
+// Blocks of BAND_NT threads per SM the band kernel is compiled for (its
+// register budget: 65536 / (BAND_NT * blocks) per thread).
 template <typename T>
-__global__ void __launch_bounds__(256) step3d_band(StepParams<T> P) {
-  const int blk = blockIdx.x;
-  if (blk == 0 && P.do_rim && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
-  int b = 0;
-  while (b + 1 < P.nbox && blk >= P.box_blk[b + 1]) ++b;
-  const Box B = P.box[b];
-  const int zc = P.shell_zchunk;
-  int r = blk - P.box_blk[b];
-  const int gx = (B.x1 - B.x0 + 32) / 32, gy = (B.y1 - B.y0 + 8) / 8;
-  const int tbx = r % gx;
-  r /= gx;
-  const int tby = r % gy;
-  const int k0 = B.z0 + (r / gy) * zc;
-  const int k1 = min(k0 + zc, B.z1 + 1);
-  const int i = B.x0 + tbx * 32 + threadIdx.x, j = B.y0 + tby * 8 + threadIdx.y;
-  const bool valid = i <= B.x1 && j <= B.y1;
-  const int nx = P.nx, ny = P.ny, nz = P.nz, halo = P.halo;
-  const int64_t px = P.px, plane = px * ny;
-  int64_t o = (int64_t)i + px * j + plane * k0;
+struct BandOcc {
+  static constexpr int blocks = sizeof(T) == 4 ? 4 : 2;
+};
+
+// Coefficients of entry q from the left side's arrays L: hq = half-grid index
+// of ψ[q] (q, or q + halo + 1 on the right), g = on-grid index of q - 1
+// (q - 1, or q - 1 + halo on the right).
+template <typename T>
+__device__ __forceinline__ BandCoef<T> coef_at(const BandSide<T>& L, int hq, int g) {
+  return BandCoef<T>{__ldg(L.bKh + hq), __ldg(L.ah + hq), __ldg(L.bKh + hq - 1),
+                     __ldg(L.ah + hq - 1), __ldg(L.bK + g), __ldg(L.a + g)};
+}
+
+// Band state of one column along x or y: side (0 none), entry q, first
+// flag; for the slab's own axis also the offsets of ψ[q] and ξ[q-1] at the
+// current plane (side folded in) and the coefficients, held along the column.
+// Columns that lie in an x or y band only at the edge of another slab
+// recompute their offsets per plane, so the state they keep is small.
+template <typename I>
+struct ColBand {
+  int s = 0, q = 0;
+  bool first = false;
+  I pq = 0, xq = 0;
+};
+
+template <typename T, typename I, int KIND>
+__device__ __forceinline__ void band_body(const StepParams<T>& P, int blk, const Box& B, int r) {
+  constexpr bool GEN = KIND == 15;
+  constexpr bool XPRIM = KIND == 1, YPRIM = KIND == 3;  // the slab's own axis
+  const int W = B.x1 - B.x0 + 1;
+  const int ncol = W * (B.y1 - B.y0 + 1);
+  const int ncb = (ncol + BAND_NT - 1) / BAND_NT;
+  const int l = (r % ncb) * BAND_NT + (int)threadIdx.x;
+  const int k0 = B.z0 + (r / ncb) * P.shell_zchunk;
+  const int k1 = min(k0 + P.shell_zchunk, B.z1 + 1);
+  const bool valid = l < ncol;
+  const int i = B.x0 + (valid ? l % W : 0), j = B.y0 + (valid ? l / W : 0);
+  const int halo = P.halo;
+  const I px = (I)P.px, plane = (I)P.plane;
+  const I col = (I)i + px * (I)j;
+  I o = col + plane * (I)k0;
   int ioe = P.io.blk_off[blk];
   const int ioe1 = P.io.blk_off[blk + 1];
-  const int local = threadIdx.x + 32 * threadIdx.y;
-  // x and y band of the column (fixed along z): side, entry q, first flag,
-  // and the element offsets of ψ[q] and ξ[q-1] at the current plane
-  int sx = 0, sy = 0, qx = 0, qy = 0;
-  bool fx = false, fy = false;
-  int64_t pqx = 0, xqx = 0, pqy = 0, xqy = 0;
-  if (valid) {
-    sx = band_of(i, nx, halo, P.first_r[0], qx, fx);
-    if (sx != 0 && !P.active[0][sx - 1]) sx = 0;
-    sy = band_of(j, ny, halo, P.first_r[1], qy, fy);
-    if (sy != 0 && !P.active[1][sy - 1]) sy = 0;
-    const int64_t jk = (int64_t)j + (int64_t)ny * k0;
-    pqx = (int64_t)(halo + 1) * jk + qx;
-    xqx = (int64_t)halo * jk + (qx - 1);
-    pqy = (int64_t)i + px * (qy + (int64_t)(halo + 1) * k0);
-    xqy = (int64_t)i + px * ((qy - 1) + (int64_t)halo * k0);
+  const BandSide<T>&LX = P.band[0][0], &LY = P.band[1][0], &LZ = P.band[2][0];
+  ColBand<I> X, Y;
+  BandCoef<T> cx{}, cy{};
+  if ((KIND & 1) && valid) {
+    X.s = band_of(i, P.nx, halo, P.first_r[0], X.q, X.first);
+    if (!XPRIM && X.s != 0 && !(X.s == 1 ? P.active[0][0] : P.active[0][1])) X.s = 0;
+    if (XPRIM) {
+      const bool R = X.s == 2;
+      const I jk = (I)j + (I)P.ny * (I)k0;
+      X.pq = (I)(halo + 1) * jk + (I)X.q + (R ? (I)P.psi_side[0] : (I)0);
+      X.xq = (I)halo * jk + (I)(X.q - 1) + (R ? (I)P.xi_side[0] : (I)0);
+      cx = coef_at(LX, X.q + (R ? halo + 1 : 0), X.q - 1 + (R ? halo : 0));
+    }
   }
-  const int64_t stx_p = (int64_t)(halo + 1) * ny, stx_x = (int64_t)halo * ny;
-  const int64_t sty_p = px * (halo + 1), sty_x = px * halo;
+  if ((KIND & 2) && valid) {
+    Y.s = band_of(j, P.ny, halo, P.first_r[1], Y.q, Y.first);
+    if (!YPRIM && Y.s != 0 && !(Y.s == 1 ? P.active[1][0] : P.active[1][1])) Y.s = 0;
+    if (YPRIM) {
+      const bool R = Y.s == 2;
+      Y.pq = (I)i + px * ((I)Y.q + (I)(halo + 1) * (I)k0) + (R ? (I)P.psi_side[1] : (I)0);
+      Y.xq = (I)i + px * ((I)(Y.q - 1) + (I)halo * (I)k0) + (R ? (I)P.xi_side[1] : (I)0);
+      cy = coef_at(LY, Y.q + (R ? halo + 1 : 0), Y.q - 1 + (R ? halo : 0));
+    }
+  }
+  // z slab: ψ[q] of node (i, j, k) at o - zsp and ξ[q-1] at o - plane - zsx
+  // (zs = plane * (k - q) less the side offset)
+  I zsp = 0, zsx = 0;
+  if (KIND == 7 && B.z0 != 1) {
+    const I zs = plane * (I)(P.nz - halo - 2);
+    zsp = zs - (I)P.psi_side[2];
+    zsx = zs - (I)P.xi_side[2];
+  }
   const T* __restrict__ pcur = P.pcur;
   T pm = 0, pc = 0, pp = 0;
   if (valid) {
-    pm = __ldg(pcur + o - plane);
+    pm = __ldg(pcur + (o - plane));
     pc = __ldg(pcur + o);
   }
-  const int64_t col = (int64_t)i + px * j;
-  for (int k = k0; k < k1; ++k, o += plane, pqx += stx_p, xqx += stx_x, pqy += sty_p,
-           xqy += sty_x) {
+  T zsq = 0;  // new ψ on the upper z face of the previous plane's node
+  for (int k = k0; k < k1; ++k, o += plane) {
+    // z band of the plane (uniform over the block)
+    int sz = 0, qz = 0;
+    bool fz = false;
+    if (KIND & 4) {
+      sz = band_of(k, P.nz, halo, P.first_r[2], qz, fz);
+      if (GEN && sz != 0 && !(sz == 1 ? P.active[2][0] : P.active[2][1])) sz = 0;
+    }
+    const bool zR = sz == 2;
+    const bool zcarry = k > k0 && !fz;
     T v = 0;
     if (valid) {
-      pp = __ldg(pcur + o + plane);
+      pp = __ldg(pcur + (o + plane));
       const T po = __ldg(P.pold + o), f = __ldg(P.fact + o);
+      // offsets of this plane's x and y entries
+      I xpq = X.pq, xxq = X.xq, ypq = Y.pq, yxq = Y.xq;
+      if ((KIND & 1) && !XPRIM && X.s) {
+        const bool R = X.s == 2;
+        const I jk = (I)j + (I)P.ny * (I)k;
+        xpq = (I)(halo + 1) * jk + (I)X.q + (R ? (I)P.psi_side[0] : (I)0);
+        xxq = (I)halo * jk + (I)(X.q - 1) + (R ? (I)P.xi_side[0] : (I)0);
+      }
+      if ((KIND & 2) && !YPRIM && Y.s) {
+        const bool R = Y.s == 2;
+        ypq = (I)i + px * ((I)Y.q + (I)(halo + 1) * (I)k) + (R ? (I)P.psi_side[1] : (I)0);
+        yxq = (I)i + px * ((I)(Y.q - 1) + (I)halo * (I)k) + (R ? (I)P.xi_side[1] : (I)0);
+      }
       // band values of this plane, issued before the arithmetic
       T xq = 0, xmq = 0, xx = 0, yq = 0, ymq = 0, yx = 0, zq = 0, zmq = 0, zx = 0;
-      if (sx) {
-        const BandSide<T>& B = P.band[0][sx - 1];
-        xq = B.psi_old[pqx];
-        xmq = B.psi_old[pqx - 1];
-        xx = B.xi[xqx];
+      if ((KIND & 1) && X.s) {
+        xq = LX.psi_old[xpq];
+        xmq = LX.psi_old[xpq - 1];
+        xx = LX.xi[xxq];
       }
-      if (sy) {
-        const BandSide<T>& B = P.band[1][sy - 1];
-        yq = B.psi_old[pqy];
-        ymq = B.psi_old[pqy - px];
-        yx = B.xi[xqy];
+      if ((KIND & 2) && Y.s) {
+        yq = LY.psi_old[ypq];
+        ymq = LY.psi_old[ypq - px];
+        yx = LY.xi[yxq];
       }
-      int qz;
-      bool fz;
-      int sz = band_of(k, nz, halo, P.first_r[2], qz, fz);
-      if (sz != 0 && !P.active[2][sz - 1]) sz = 0;
-      if (sz) {
-        const BandSide<T>& B = P.band[2][sz - 1];
-        zq = B.psi_old[col + plane * qz];
-        zmq = B.psi_old[col + plane * (qz - 1)];
-        zx = B.xi[col + plane * (qz - 1)];
+      I zp = o - zsp, zxo = o - plane - zsx;
+      if (GEN) {
+        zp = col + plane * (I)qz + (zR ? (I)P.psi_side[2] : (I)0);
+        zxo = col + plane * (I)(qz - 1) + (zR ? (I)P.xi_side[2] : (I)0);
       }
-      const T xm = __ldg(pcur + o - 1), xp = __ldg(pcur + o + 1);
-      const T ym = __ldg(pcur + o - px), yp = __ldg(pcur + o + px);
+      if ((KIND & 4) && sz) {
+        zq = LZ.psi_old[zp];
+        if (!zcarry) zmq = LZ.psi_old[zp - plane];
+        zx = LZ.xi[zxo];
+      }
+      const T xm = __ldg(pcur + (o - 1)), xp = __ldg(pcur + (o + 1));
+      const T ym = __ldg(pcur + (o - px)), yp = __ldg(pcur + (o + px));
       const T d2x = second_diff(xm, pc, xp, P.inv_d2[0]);
       const T d2y = second_diff(ym, pc, yp, P.inv_d2[1]);
       const T d2z = second_diff(pm, pc, pp, P.inv_d2[2]);
       v = leapfrog3d(pc, po, f, d2x, d2y, d2z);
       T damp = 0;
-      if (sx)
-        band_apply(P.band[0][sx - 1], qx, fx, pqx, (int64_t)1, xqx, xq, xmq, xx, xm, pc, xp, d2x,
-                   f, P.inv_d[0], damp);
-      if (sy)
-        band_apply(P.band[1][sy - 1], qy, fy, pqy, px, xqy, yq, ymq, yx, ym, pc, yp, d2y, f,
-                   P.inv_d[1], damp);
-      if (sz)
-        band_apply(P.band[2][sz - 1], qz, fz, col + plane * qz, plane, col + plane * (qz - 1), zq,
-                   zmq, zx, pm, pc, pp, d2z, f, P.inv_d[2], damp);
+      if ((KIND & 1) && X.s) {
+        const bool R = X.s == 2;
+        band_apply(LX, XPRIM ? cx : coef_at(LX, X.q + (R ? halo + 1 : 0), X.q - 1 + (R ? halo : 0)),
+                   X.first, xpq, (I)1, xxq, xq, xmq, xx, xm, pc, xp, d2x, f, P.inv_d[0], damp);
+      }
+      if ((KIND & 2) && Y.s) {
+        const bool R = Y.s == 2;
+        band_apply(LY, YPRIM ? cy : coef_at(LY, Y.q + (R ? halo + 1 : 0), Y.q - 1 + (R ? halo : 0)),
+                   Y.first, ypq, px, yxq, yq, ymq, yx, ym, pc, yp, d2y, f, P.inv_d[1], damp);
+      }
+      if ((KIND & 4) && sz) {
+        const T inv = P.inv_d[2];
+        const int hq = qz + (zR ? halo + 1 : 0), g = qz - 1 + (zR ? halo : 0);
+        const T sq = psi_face(__ldg(LZ.bKh + hq), __ldg(LZ.ah + hq), zq, pp - pc, inv);
+        const T sm = zcarry ? zsq
+                            : psi_face(__ldg(LZ.bKh + hq - 1), __ldg(LZ.ah + hq - 1), zmq,
+                                       pc - pm, inv);
+        T xn;
+        cpml_tail(__ldg(LZ.bK + g), __ldg(LZ.a + g), sq, sm, zx, d2z, f, inv, xn, damp);
+        LZ.psi_new[zp] = sq;
+        if (fz) LZ.psi_new[zp - plane] = sm;
+        LZ.xi[zxo] = xn;
+        zsq = sq;
+      }
       v += damp;
     }
     // sources and receivers of this plane (block-uniform walk)
     for (; ioe < ioe1; ++ioe) {
       const int4 en = P.io.ent[ioe];
       if (en.y != k) break;
-      if (valid && en.x == local) v = node_io(P.io, P.it, en.z, en.w, v);
+      if (valid && en.x == (int)threadIdx.x) v = node_io(P.io, P.it, en.z, en.w, v);
     }
     if (valid) P.pnew[o] = v;
     pm = pc;
     pc = pp;
+    if (XPRIM) {
+      X.pq += (I)P.psi_dz[0];
+      X.xq += (I)P.xi_dz[0];
+    }
+    if (YPRIM) {
+      Y.pq += (I)P.psi_dz[1];
+      Y.xq += (I)P.xi_dz[1];
+    }
   }
+}
+
+template <typename T, typename I>
+__global__ void __launch_bounds__(BAND_NT, BandOcc<T>::blocks) step3d_band(StepParams<T> P) {
+  const int blk = (int)blockIdx.x;
+  if (blk == 0 && P.do_rim && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
+  int b = 0;
+  while (b + 1 < P.nbox && blk >= P.box_blk[b + 1]) ++b;
+  const Box B = P.box[b];
+  const int r = blk - P.box_blk[b];
+  if (B.kind == 1)
+    band_body<T, I, 1>(P, blk, B, r);
+  else if (B.kind == 3)
+    band_body<T, I, 3>(P, blk, B, r);
+  else if (B.kind == 7)
+    band_body<T, I, 7>(P, blk, B, r);
+  else
+    band_body<T, I, 15>(P, blk, B, r);
 }
 
 // ---------------------------------------------------------------------------
