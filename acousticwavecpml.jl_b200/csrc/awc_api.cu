@@ -628,8 +628,8 @@ int ensure_io(awc_plan* P) {
     if (P->has_core && i >= Cb.x0 && i <= Cb.x1 && j >= Cb.y0 && j <= Cb.y1 && k >= Cb.z0 &&
         k <= Cb.z1) {
       const int64_t lx = (i - P->core_x) % 64, ly = (j - Cb.y0) % P->by;
-      const int64_t blk = (i - P->core_x) / 64 +
-                          g.x * ((j - Cb.y0) / P->by + (int64_t)g.y * ((k - Cb.z0) / P->zchunk));
+      const int64_t blk = (k - Cb.z0) / P->zchunk +
+                          g.z * ((i - P->core_x) / 64 + (int64_t)g.x * ((j - Cb.y0) / P->by));
       const int local = (int)(lx + 64 * ly);
       ent[0].push_back({{blk, (k << 32) | local}, make_int4(local, (int)k, e.sgrp, e.rgrp)});
       continue;

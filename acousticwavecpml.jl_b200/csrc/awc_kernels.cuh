@@ -336,11 +336,15 @@ __global__ void __launch_bounds__(32 * TY) step3d_core(const __grid_constant__ C
   uint64_t* empty = full + S;
   volatile int* abort = reinterpret_cast<volatile int*>(empty + S);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
+  // blocks are numbered z chunk fastest, so the chunks of one column tile run
+  // together and the planes they share come from L2
   const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (blk == 0 && P.do_rim && P.io.nrim > 0) rim_io(P.io, P.pnew, P.it);
   const Box C = P.core;
-  const int x0 = P.core_x + blockIdx.x * L::TX, y0 = C.y0 + blockIdx.y * L::RY;
-  const int k0 = C.z0 + blockIdx.z * P.zchunk;
+  const int gz = gridDim.z, gx = gridDim.x;
+  const int bz = blk % gz, bx = (blk / gz) % gx, by = blk / (gz * gx);
+  const int x0 = P.core_x + bx * L::TX, y0 = C.y0 + by * L::RY;
+  const int k0 = C.z0 + bz * P.zchunk;
   int k1 = k0 + P.zchunk;
   if (k1 > C.z1 + 1) k1 = C.z1 + 1;
   if (k0 >= k1) return;  // block-uniform
