@@ -511,13 +511,13 @@ __device__ __forceinline__ void band_apply(const BandSide<T>& B, const BandCoef<
 // lower face is the value the column computed on the previous plane's upper
 // face (the same operations on the same operands), so it is carried instead
 // of recomputed.
-constexpr int BAND_NT = 256;
+constexpr int BAND_NT = 128;
 
 // Blocks of BAND_NT threads per SM the band kernel is compiled for (its
 // register budget: 65536 / (BAND_NT * blocks) per thread).
 template <typename T>
 struct BandOcc {
-  static constexpr int blocks = sizeof(T) == 4 ? 4 : 2;
+  static constexpr int blocks = (sizeof(T) == 4 ? 1024 : 512) / BAND_NT;
 };
 
 // Coefficients of entry q from the left side's arrays L: hq = half-grid index
