@@ -1286,7 +1286,7 @@ int awc_plan_autotune(awc_plan* P, int64_t steps, float* best_ms_per_step) {
   // phase 2: z planes per block of the band kernel
   if (P->nbox > 0) {
     int32_t wz = P->szc;
-    for (int32_t zc : {5, 10, 20, 40}) {
+    for (int32_t zc : {4, 6, 8, 10, 12, 16, 20, 32}) {
       P->szc = zc;
       box_blocks(P);
       float per = 0.f;
