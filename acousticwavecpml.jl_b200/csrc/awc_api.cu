@@ -139,23 +139,6 @@ int64_t node_of(const awc_problem* p, int64_t px, const int64_t* pos, int64_t cn
   return i + px * (j + p->ny * k);
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
-// dependency on libcuda).
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    cudaGetLastError();
-  });
-  return fn;
-}
-
 // Pipeline depth of the 3D core kernel: S stages let the TMA loads run S-3
 // planes ahead of the plane being computed. Five stages (two planes ahead)
 // measured best with the 64 x 4 tiles the autotuner picks on large grids:
@@ -694,7 +677,7 @@ int ensure_maps(awc_plan* P) {
   if (P->maps_by == P->by) return AWC_OK;
   awc_ctx* C = P->ctx;
   const awc_problem* p = &P->p;
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  PFN_cuTensorMapEncodeTiled_v12000 enc = awc::tensor_map_encoder();
   if (!enc) return set_err(&C->err, AWC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
   const bool f64 = p->precision == AWC_F64;
   const CUtensorMapDataType dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -940,6 +923,21 @@ int check_device_flag(awc_plan* P) {
 }  // namespace
 
 namespace awc {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
 // Sets the calling thread's last error (awc_last_error(NULL)) for entry
 // points defined in other translation units.
 void record_error(const char* msg) { g_thread_err = msg; }

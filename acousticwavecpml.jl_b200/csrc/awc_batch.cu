@@ -58,7 +58,7 @@ struct awc_batch {
     int64_t max_tiles;
   };
   std::vector<ShotMem> sm;
-  size_t descs = 0, tile_start = 0;
+  size_t descs = 0, tile_start = 0, maps = 0, err = 0;
   // per-shot source/receiver nodes (pitched index, groups)
   std::vector<std::vector<awc::IoRim>> io_nodes;
   // launch shape
@@ -128,8 +128,71 @@ void to_T(const double* src, std::vector<unsigned char>& out, int64_t n) {
   for (int64_t c = 0; c < n; ++c) d[c] = (T)src[c];
 }
 
+// Tile heights 4, 8 and 16 run the TMA-fed kernel on tiles 64 nodes wide;
+// 32 and 64 the register-strip kernel on tiles 32 nodes wide.
+bool tma_tiles(int ty) { return ty <= 16; }
+int64_t tile_w(int ty) { return tma_tiles(ty) ? 64 : 32; }
+int64_t tiles_x(const awc_problem& p, int ty) { return (p.nx - 2) / tile_w(ty) + 1; }
 int64_t tiles_of(const awc_problem& p, int ty) {
-  return ((p.nx - 2) / 32 + 1) * ((p.ny - 2 + ty - 1) / ty);
+  return tiles_x(p, ty) * ((p.ny - 2 + ty - 1) / ty);
+}
+
+constexpr int kBatchStages = 4;  // TMA stages: tiles loaded up to 3 ahead
+
+template <typename T, int RR>
+constexpr int batch_smem() {
+  return kBatchStages * awc::BatchTile<T, RR>::BYTES + 2 * kBatchStages * 8 + 16;
+}
+
+// Tensor maps of every shot for tile height ty (TMA kernel): dims (nx, ny),
+// pitched rows; pcur box (64 + 2A) x (ty + 2), pold and fact boxes 64 x ty.
+template <typename T>
+int build_maps(awc_batch* B, int ty) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = awc::tensor_map_encoder();
+  if (!enc) return awc::fail(B->ctx, AWC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const CUtensorMapDataType dt =
+      sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint32_t A = 16 / (cuuint32_t)sizeof(T);
+  const cuuint32_t box_c[2] = {64 + 2 * A, (cuuint32_t)ty + 2}, box_i[2] = {64, (cuuint32_t)ty};
+  const cuuint32_t es[2] = {1, 1};
+  std::vector<awc::ShotMaps> maps(B->nshots);
+  for (int32_t s = 0; s < B->nshots; ++s) {
+    const awc_problem& p = B->models[B->shots[s].model];
+    const cuuint64_t dims[2] = {(cuuint64_t)p.nx, (cuuint64_t)p.ny};
+    const cuuint64_t strides[1] = {(cuuint64_t)(pitch32(p.nx) * sizeof(T))};
+    auto make = [&](CUtensorMap* m, void* base, const cuuint32_t* box) {
+      return enc(m, dt, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    };
+    const auto& M = B->sm[s];
+    for (int b = 0; b < 3; ++b)
+      if (!make(&maps[s].c[b], B->arena + M.buf[b], box_c) ||
+          !make(&maps[s].o[b], B->arena + M.buf[b], box_i))
+        return awc::fail(B->ctx, AWC_ERR_CUDA, "tensor map encoding failed");
+    if (!make(&maps[s].f, B->arena + B->m_fact[B->shots[s].model], box_i))
+      return awc::fail(B->ctx, AWC_ERR_CUDA, "tensor map encoding failed");
+  }
+  BATCH_TRY(B->ctx, cudaMemcpyAsync(B->arena + B->maps, maps.data(), maps.size() * sizeof(maps[0]),
+                                    cudaMemcpyHostToDevice, B->ctx->stream));
+  BATCH_TRY(B->ctx, cudaStreamSynchronize(B->ctx->stream));
+  return AWC_OK;
+}
+
+// Opts the TMA kernels into their dynamic shared memory (once per process).
+int init_batch_attrs(awc_ctx* C) {
+#define AWC_BATTR(T, RR)                                                                   \
+  BATCH_TRY(C, cudaFuncSetAttribute(awc::step2d_batch_tma<T, RR, kBatchStages>,             \
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,           \
+                                    batch_smem<T, RR>()))
+  AWC_BATTR(float, 1);
+  AWC_BATTR(float, 2);
+  AWC_BATTR(float, 4);
+  AWC_BATTR(double, 1);
+  AWC_BATTR(double, 2);
+  AWC_BATTR(double, 4);
+#undef AWC_BATTR
+  return AWC_OK;
 }
 
 // Device descriptors and per-tile source/receiver lists for tile height ty.
@@ -150,7 +213,7 @@ int build_layout(awc_batch* B) {
     D.nx = (int32_t)p.nx;
     D.ny = (int32_t)p.ny;
     D.halo = p.halo;
-    D.gx = (int32_t)((p.nx - 2) / 32 + 1);
+    D.gx = (int32_t)tiles_x(p, ty);
     const double d[2] = {p.dx, p.dy};
     for (int a = 0; a < 2; ++a) {
       D.inv_d[a] = (T)(1.0 / d[a]);
@@ -177,7 +240,7 @@ int build_layout(awc_batch* B) {
     }
     // sources and receivers: rim nodes to the shot's rim list (tile 0),
     // interior nodes to their tile, (tile, local) order
-    const int64_t px = pitch32(p.nx), gx = (p.nx - 2) / 32 + 1;
+    const int64_t px = pitch32(p.nx), gx = tiles_x(p, ty), W = tile_w(ty);
     const int64_t nt_tiles = tiles_of(p, ty);
     std::vector<awc::IoRim> rim;
     std::vector<std::pair<int64_t, int4>> ent;
@@ -187,8 +250,8 @@ int build_layout(awc_batch* B) {
         rim.push_back(e);
         continue;
       }
-      const int64_t tile = i / 32 + gx * ((j - 1) / ty);
-      const int local = (int)(i % 32 + 32 * ((j - 1) % ty));
+      const int64_t tile = i / W + gx * ((j - 1) / ty);
+      const int local = (int)(i % W + W * ((j - 1) % ty));
       ent.push_back({tile * 4096 + local, make_int4(local, 0, e.sgrp, e.rgrp)});
     }
     std::sort(ent.begin(), ent.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
@@ -229,6 +292,10 @@ int build_layout(awc_batch* B) {
   BATCH_TRY(C, cudaMemcpyAsync(B->arena + B->tile_start, tile_start.data(), tile_start.size() * 4,
                                cudaMemcpyHostToDevice, C->stream));
   BATCH_TRY(C, cudaStreamSynchronize(C->stream));
+  if (tma_tiles(ty)) {
+    const int rc = build_maps<T>(B, ty);
+    if (rc) return rc;
+  }
   B->ntiles = tile_start[B->nshots];
   B->io_ty = ty;
   return AWC_OK;
@@ -237,13 +304,11 @@ int build_layout(awc_batch* B) {
 template <typename T>
 using BatchKernel = void (*)(const awc::ShotDesc<T>*, const int32_t*, int32_t, int32_t, int32_t);
 
-// Tile height -> kernel: 4 warps per block, each streaming tile_y / 4 rows.
+// Tile height 32 or 64 -> register-strip kernel: 4 warps per block, each
+// streaming tile_y / 4 rows.
 template <typename T>
 BatchKernel<T> batch_kernel(int tile_y) {
   switch (tile_y) {
-    case 4: return awc::step2d_batch<T, 4, 1>;
-    case 8: return awc::step2d_batch<T, 4, 2>;
-    case 16: return awc::step2d_batch<T, 4, 4>;
     case 32: return awc::step2d_batch<T, 4, 8>;
     case 64: return awc::step2d_batch<T, 4, 16>;
     default: return nullptr;
@@ -251,10 +316,38 @@ BatchKernel<T> batch_kernel(int tile_y) {
 }
 
 template <typename T>
+using BatchTmaKernel = void (*)(const awc::ShotDesc<T>*, const awc::ShotMaps*, const int32_t*,
+                                int32_t, int32_t, int32_t, int32_t*);
+
+template <typename T>
 int launch_batch_step(awc_batch* B, int64_t it, cudaStream_t st) {
+  const auto* D = (const awc::ShotDesc<T>*)(B->arena + B->descs);
+  const auto* ts = (const int32_t*)(B->arena + B->tile_start);
+  int& occ = B->occ[B->ty];
+  if (tma_tiles(B->ty)) {
+    // tile_y rows = BATCH_CW consumer warps x RR rows each, plus a producer warp
+    BatchTmaKernel<T> k = nullptr;
+    int smem = 0;
+    const int warps = awc::BATCH_CW + 1;
+    switch (B->ty) {
+      case 4: k = awc::step2d_batch_tma<T, 1, kBatchStages>; smem = batch_smem<T, 1>(); break;
+      case 8: k = awc::step2d_batch_tma<T, 2, kBatchStages>; smem = batch_smem<T, 2>(); break;
+      default: k = awc::step2d_batch_tma<T, 4, kBatchStages>; smem = batch_smem<T, 4>(); break;
+    }
+    if (occ == 0) {
+      BATCH_TRY(B->ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 32 * warps, smem));
+      occ = std::max(occ, 1);
+    }
+    const int per_sm = std::min<int>(B->bps, occ);
+    const int grid = std::max(1, std::min(B->ntiles, B->ctx->num_sms * per_sm));
+    k<<<grid, dim3(32, warps), smem, st>>>(D, (const awc::ShotMaps*)(B->arena + B->maps), ts,
+                                          B->nshots, B->ntiles, (int)it,
+                                          (int32_t*)(B->arena + B->err));
+    BATCH_TRY(B->ctx, cudaGetLastError());
+    return AWC_OK;
+  }
   const BatchKernel<T> k = batch_kernel<T>(B->ty);
   if (!k) return awc::fail(B->ctx, AWC_ERR_INVALID, "unsupported tile height");
-  int& occ = B->occ[B->ty];
   if (occ == 0) {
     BATCH_TRY(B->ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, 0));
     occ = std::max(occ, 1);
@@ -262,8 +355,6 @@ int launch_batch_step(awc_batch* B, int64_t it, cudaStream_t st) {
   // a persistent grid: never more blocks than can be resident at once
   const int per_sm = std::min<int>(B->bps, occ);
   const int grid = std::max(1, std::min(B->ntiles, B->ctx->num_sms * per_sm));
-  const auto* D = (const awc::ShotDesc<T>*)(B->arena + B->descs);
-  const auto* ts = (const int32_t*)(B->arena + B->tile_start);
   k<<<grid, dim3(32, 4), 0, st>>>(D, ts, B->nshots, B->ntiles, (int)it);
   BATCH_TRY(B->ctx, cudaGetLastError());
   return AWC_OK;
@@ -343,7 +434,8 @@ int awc_batch_create(awc_ctx* C, int32_t nmodels, const awc_problem* models,
     M.rec_off = take((nr + 1) * 4);
     M.rec_ids = take(nr * 4);
     M.rim = take((ns + nr) * sizeof(awc::IoRim));
-    M.max_tiles = tiles_of(p, 4);
+    M.max_tiles = 0;  // per-tile list bounds for the most numerous tiles of any height
+    for (int t : {4, 8, 16, 32, 64}) M.max_tiles = std::max(M.max_tiles, tiles_of(p, t));
     M.blk_off = take((M.max_tiles + 1) * 4);
     M.ent = take((ns + nr) * sizeof(int4));
     M.coef = take(2 * (8 * h + 4) * esz);
@@ -352,6 +444,8 @@ int awc_batch_create(awc_ctx* C, int32_t nmodels, const awc_problem* models,
     staging = std::max<int64_t>(staging, nt * nr);
   }
   B->descs = take(nshots * std::max(sizeof(awc::ShotDesc<float>), sizeof(awc::ShotDesc<double>)));
+  B->maps = take(nshots * sizeof(awc::ShotMaps));
+  B->err = take(16);
   B->tile_start = take((nshots + 1) * 4);
   const size_t o_staging = take(staging * 8);
   B->staging_len = staging;
@@ -365,6 +459,10 @@ int awc_batch_create(awc_ctx* C, int32_t nmodels, const awc_problem* models,
   }
   B->staging = (double*)(B->arena + o_staging);
   cudaStream_t st = C->stream;
+  if (cudaMemsetAsync(B->arena + B->err, 0, 4, st) != cudaSuccess || init_batch_attrs(C)) {
+    delete B;
+    return awc::fail(C, AWC_ERR_CUDA, "batch setup failed");
+  }
   std::vector<unsigned char> tmp;
   auto up = [&](size_t at, const void* src, size_t bytes) {
     return cudaMemcpyAsync(B->arena + at, src, bytes, cudaMemcpyHostToDevice, st);
@@ -556,6 +654,13 @@ int awc_batch_run(awc_batch* B, int64_t nsteps, int32_t use_graph, float* ms) {
   BATCH_TRY(C, cudaEventSynchronize(C->ev1));
   if (ms) BATCH_TRY(C, cudaEventElapsedTime(ms, C->ev0, C->ev1));
   B->step += n;
+  // a bounded wait of the TMA kernel that ran out
+  int32_t flag = 0;
+  BATCH_TRY(C, cudaMemcpy(&flag, B->arena + B->err, 4, cudaMemcpyDeviceToHost));
+  if (flag) {
+    BATCH_TRY(C, cudaMemset(B->arena + B->err, 0, 4));
+    return awc::fail(C, AWC_ERR_TIMEOUT, "a bounded wait on a pipeline barrier ran out");
+  }
   return AWC_OK;
 }
 

@@ -1,6 +1,8 @@
 // awc_ctx.h — the context object shared by the translation units of
 // libawcpml (internal; the public API sees it as an opaque handle).
 #pragma once
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -49,4 +51,8 @@ void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t coun
 // Sets the calling thread's last error (awc_last_error(NULL)) and, when ctx
 // is not NULL, the context's; returns code.
 int fail(awc_ctx* ctx, int code, const char* msg);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda); NULL when the driver does not offer it.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 }  // namespace awc

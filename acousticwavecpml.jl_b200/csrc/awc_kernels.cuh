@@ -225,13 +225,16 @@ __device__ __forceinline__ T node_io(const Io<T>& io, int it, int sgrp, int rgrp
 
 // Rim nodes of the step (block 0 only): pnew[rim] += sources, then sample.
 template <typename T>
-__device__ __forceinline__ void rim_io(const Io<T>& io, T* pnew, int it) {
-  const int t = threadIdx.x + blockDim.x * threadIdx.y;
-  const int nt = blockDim.x * blockDim.y;
+__device__ __forceinline__ void rim_io(const Io<T>& io, T* pnew, int it, int t, int nt) {
   for (int e = t; e < io.nrim; e += nt) {
     const IoRim r = io.rim[e];
     pnew[r.node] = node_io(io, it, r.sgrp, r.rgrp, pnew[r.node]);
   }
+}
+template <typename T>
+__device__ __forceinline__ void rim_io(const Io<T>& io, T* pnew, int it) {
+  rim_io(io, pnew, it, (int)(threadIdx.x + blockDim.x * threadIdx.y),
+         (int)(blockDim.x * blockDim.y));
 }
 
 // ---------------------------------------------------------------------------
@@ -281,6 +284,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
       " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+// 2D tiled TMA load of one box into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
+                                            int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
       : "memory");
 }
 
@@ -890,6 +903,254 @@ __global__ void __launch_bounds__(32 * TY) step2d_batch(const ShotDesc<T>* __res
         if (en.x == lidx) v = node_io(D.io, it, en.z, en.w, v);
       }
       pnew[o] = v;
+    }
+  }
+}
+
+// Tensor maps of one batched shot (in global memory, 64-byte aligned): for
+// each rotating field buffer a map with the pcur box ((64 + 2A) x (RY + 2))
+// and one with the inner box (64 x RY), and the map of its model's fact.
+struct ShotMaps {
+  CUtensorMap c[3];
+  CUtensorMap o[3];
+  CUtensorMap f;
+};
+
+// Batched 2D shots, TMA-fed: the same persistent walk of the global tile list
+// as step2d_batch, with tiles of 64 x (4 RR) nodes. A block has CW = 4
+// consumer warps and one producer warp. The producer's lane 0 streams the
+// block's tiles through S shared-memory stages, up to S tiles ahead: for each
+// tile it writes a header (shot, tile origin, the shot's sizes, its output
+// field, whether the tile meets a CPML band, the tile's source/receiver list
+// bounds) and issues cp.async.bulk.tensor loads of the pcur box with a
+// one-node ring and of the pold and fact boxes from the shot's tensor maps.
+// Each stage has a "full" mbarrier (the header arrival and the TMA bytes) and
+// an "empty" one (one arrival per consumer warp once its values are in
+// registers). Consumer lane l of warp w owns nodes x0 + 2l, x0 + 2l + 1 of
+// rows y0 + w RR .. y0 + w RR + RR - 1. Band nodes and sources/receivers take
+// the same per-node code as step2d_batch, so every shot computes bitwise
+// what its single-shot run computes. Waits are bounded: a wait that runs out
+// sets *err and ends the block.
+constexpr int BATCH_CW = 4;  // consumer warps of the TMA batched kernel
+
+template <typename T>
+struct TileHdr {
+  int32_t shot, local, x0, y0;
+  int32_t nx, ny, band, e0;
+  int32_t e1, rim;
+  int64_t px;
+  T* pnew;
+  T ix2, iy2;
+};
+
+template <typename T, int RR>
+struct BatchTile {
+  static constexpr int TX = 64, RY = BATCH_CW * RR;
+  static constexpr int A = 16 / (int)sizeof(T);
+  static constexpr int PW = TX + 2 * A;
+  static constexpr int PC_BYTES = PW * (RY + 2) * (int)sizeof(T);
+  static constexpr int PC_PAD = (PC_BYTES + 127) / 128 * 128;
+  static constexpr int IN_BYTES = TX * RY * (int)sizeof(T);
+  static constexpr int HDR = 128;  // header slot (TileHdr, padded)
+  static constexpr int BYTES = PC_PAD + 2 * IN_BYTES + HDR;
+};
+
+template <typename T, int RR, int S>
+__global__ void __launch_bounds__(32 * (BATCH_CW + 1))
+    step2d_batch_tma(const ShotDesc<T>* __restrict__ shots, const ShotMaps* __restrict__ maps,
+                     const int32_t* __restrict__ tile_start, int32_t nshots, int32_t ntiles,
+                     int32_t it, int32_t* err) {
+  using L = BatchTile<T, RR>;
+  using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * L::BYTES);
+  uint64_t* empty = full + S;
+  volatile int* abort = reinterpret_cast<volatile int*>(empty + S);
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int nb = (int)gridDim.x, b0 = (int)blockIdx.x;
+  const int nu = b0 < ntiles ? (ntiles - 1 - b0) / nb + 1 : 0;  // tiles of this block
+  if (nu == 0) return;  // block-uniform
+  if (w == 0 && lane == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], BATCH_CW);
+    }
+    *abort = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  const int pb = (it + 1) % 3, ob = it % 3, wb = (it + 2) % 3;
+
+  if (w == BATCH_CW) {
+    // ---- producer ----------------------------------------------------------
+    if (lane != 0) return;
+    int ps = 0;  // shot cursor (tiles of a block increase)
+    int u = 0;
+    bool ok = true;
+    for (; u < nu; ++u) {
+      const int s = u % S;
+      if (u >= S && !mbar_wait(&empty[s], ((u / S) + 1) & 1, abort)) {
+        ok = false;
+        break;
+      }
+      const int t = b0 + u * nb;
+      while (ps + 1 < nshots && __ldg(tile_start + ps + 1) <= t) ++ps;
+      const ShotDesc<T>& D = shots[ps];
+      const int local = t - __ldg(tile_start + ps);
+      const int x0 = (local % D.gx) * L::TX, y0 = 1 + (local / D.gx) * L::RY;
+      const int nx = D.nx, ny = D.ny, halo = D.halo;
+      unsigned char* st = smem + s * L::BYTES;
+      TileHdr<T>* h = reinterpret_cast<TileHdr<T>*>(st + L::PC_PAD + 2 * L::IN_BYTES);
+      h->shot = ps;
+      h->local = local;
+      h->x0 = x0;
+      h->y0 = y0;
+      h->nx = nx;
+      h->ny = ny;
+      h->band = ((D.active[0][0] && x0 <= halo) || (D.active[0][1] && x0 + L::TX - 1 >= nx - halo - 1) ||
+                 (D.active[1][0] && y0 <= halo) || (D.active[1][1] && y0 + L::RY - 1 >= ny - halo - 1))
+                    ? 1 : 0;
+      h->e0 = D.io.blk_off[local];
+      h->e1 = D.io.blk_off[local + 1];
+      h->rim = (local == 0 && D.io.nrim > 0) ? 1 : 0;
+      h->px = D.px;
+      h->pnew = D.buf[wb];
+      h->ix2 = D.inv_d2[0];
+      h->iy2 = D.inv_d2[1];
+      const ShotMaps* M = maps + ps;
+      // the arrive that follows releases the header writes with the stage
+      mbar_expect_tx(&full[s], L::PC_BYTES + 2 * L::IN_BYTES);
+      tma_load_2d(st, &M->c[pb], &full[s], x0 - L::A, y0 - 1);
+      tma_load_2d(st + L::PC_PAD, &M->o[ob], &full[s], x0, y0);
+      tma_load_2d(st + L::PC_PAD + L::IN_BYTES, &M->f, &full[s], x0, y0);
+    }
+    if (!ok) {
+      // a wait ran out: record it and let the loads in flight land first
+      *abort = 1;
+      atomicExch(err, 1);
+      for (int v = u - S > 0 ? u - S : 0; v < u; ++v)
+        for (int n = 0; n < 64; ++n)
+          if (mbar_try_wait(&full[v % S], (v / S) & 1, 1000000u)) break;
+    }
+    return;
+  }
+
+  // ---- consumers -----------------------------------------------------------
+  const int ct = lane + 32 * w;  // consumer thread index
+  const int cbase = (w * RR + 1) * L::PW + 2 * lane + L::A;  // pcur stage index of row 0
+  const int ibase = w * RR * L::TX + 2 * lane;               // pold/fact stage index of row 0
+  for (int u = 0; u < nu; ++u) {
+    const int s = u % S;
+    if (!mbar_wait(&full[s], (u / S) & 1, abort)) {
+      *abort = 1;
+      atomicExch(err, 1);
+      return;
+    }
+    const unsigned char* st = smem + s * L::BYTES;
+    const TileHdr<T> h = *reinterpret_cast<const TileHdr<T>*>(st + L::PC_PAD + 2 * L::IN_BYTES);
+    const T* cc = reinterpret_cast<const T*>(st);
+    const T* oo = reinterpret_cast<const T*>(st + L::PC_PAD);
+    const T* ff = oo + L::TX * L::RY;
+    // rows -1 .. RR of the thread's column pair, its x aprons, pold and fact
+    V2 pcv[RR + 2];
+    T xmv[RR], xpv[RR];
+    V2 pov[RR], fv[RR];
+#pragma unroll
+    for (int r = 0; r < RR + 2; ++r)
+      pcv[r] = *reinterpret_cast<const V2*>(cc + cbase + (r - 1) * L::PW);
+#pragma unroll
+    for (int r = 0; r < RR; ++r) {
+      xmv[r] = cc[cbase + r * L::PW - 1];
+      xpv[r] = cc[cbase + r * L::PW + 2];
+      pov[r] = *reinterpret_cast<const V2*>(oo + ibase + r * L::TX);
+      fv[r] = *reinterpret_cast<const V2*>(ff + ibase + r * L::TX);
+    }
+    // this warp's values are in registers: the producer may refill the stage
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s]);
+    if (h.rim) {
+      const Io<T> io = shots[h.shot].io;
+      rim_io(io, h.pnew, it, ct, 32 * BATCH_CW);
+    }
+    const int xa = h.x0 + 2 * lane, ja = h.y0 + w * RR;
+    T v[RR][2], d2x[RR][2], d2y[RR][2];
+#pragma unroll
+    for (int r = 0; r < RR; ++r) {
+      const T pc0 = pcv[r + 1].x, pc1 = pcv[r + 1].y;
+      d2x[r][0] = second_diff(xmv[r], pc0, pc1, h.ix2);
+      d2x[r][1] = second_diff(pc0, pc1, xpv[r], h.ix2);
+      d2y[r][0] = second_diff(pcv[r].x, pc0, pcv[r + 2].x, h.iy2);
+      d2y[r][1] = second_diff(pcv[r].y, pc1, pcv[r + 2].y, h.iy2);
+      v[r][0] = leapfrog2d(pc0, pov[r].x, fv[r].x, d2x[r][0], d2y[r][0]);
+      v[r][1] = leapfrog2d(pc1, pov[r].y, fv[r].y, d2x[r][1], d2y[r][1]);
+    }
+    if (h.band) {
+      const ShotDesc<T>& D = shots[h.shot];
+      const int nx = h.nx, ny = h.ny, halo = D.halo;
+#pragma unroll
+      for (int r = 0; r < RR; ++r)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const int i = xa + c, j = ja + r;
+          if (i < 1 || i > nx - 2 || j > ny - 2) continue;
+          int q;
+          bool first;
+          const int bx = band_of(i, nx, halo, D.first_r[0], q, first);
+          const int by = band_of(j, ny, halo, D.first_r[1], q, first);
+          const bool ax = bx != 0 && D.active[0][bx - 1], ay = by != 0 && D.active[1][by - 1];
+          if (!ax && !ay) continue;
+          const T pc = c ? pcv[r + 1].y : pcv[r + 1].x;
+          const T xm = c ? pcv[r + 1].x : xmv[r], xp = c ? xpv[r] : pcv[r + 1].y;
+          const T ym = c ? pcv[r].y : pcv[r].x, yp = c ? pcv[r + 2].y : pcv[r + 2].x;
+          const T f = c ? fv[r].y : fv[r].x;
+          T damp = 0;
+          if (ax) {
+            BandSide<T> B = D.band[0][bx - 1];
+            B.psi_old = D.psi[0][bx - 1][it & 1];
+            B.psi_new = D.psi[0][bx - 1][(it + 1) & 1];
+            band_of(i, nx, halo, D.first_r[0], q, first);
+            band_axis(B, q, first, xm, pc, xp, d2x[r][c], f, D.inv_d[0], (int64_t)(halo + 1) * j,
+                      (int64_t)halo * j, (int64_t)1, damp);
+          }
+          if (ay) {
+            BandSide<T> B = D.band[1][by - 1];
+            B.psi_old = D.psi[1][by - 1][it & 1];
+            B.psi_new = D.psi[1][by - 1][(it + 1) & 1];
+            band_of(j, ny, halo, D.first_r[1], q, first);
+            band_axis(B, q, first, ym, pc, yp, d2y[r][c], f, D.inv_d[1], (int64_t)i, (int64_t)i,
+                      h.px, damp);
+          }
+          v[r][c] += damp;
+        }
+    }
+    // sources and receivers of the tile (lists are per tile, rarely non-empty)
+    if (h.e0 < h.e1) {
+      const Io<T>& io = shots[h.shot].io;
+      for (int e = h.e0; e < h.e1; ++e) {
+        const int4 en = io.ent[e];
+        const int lx = en.x % L::TX - 2 * lane, ly = en.x / L::TX - w * RR;
+        if (lx >= 0 && lx < 2 && ly >= 0 && ly < RR) {
+#pragma unroll
+          for (int r = 0; r < RR; ++r)
+            if (ly == r) {
+              if (lx == 0) v[r][0] = node_io(io, it, en.z, en.w, v[r][0]);
+              else v[r][1] = node_io(io, it, en.z, en.w, v[r][1]);
+            }
+        }
+      }
+    }
+    const bool vx0 = xa >= 1 && xa <= h.nx - 2, vx1 = xa + 1 <= h.nx - 2;
+#pragma unroll
+    for (int r = 0; r < RR; ++r) {
+      const int j = ja + r;
+      if (j > h.ny - 2) break;
+      T* row = h.pnew + h.px * j + xa;
+      if (vx0 && vx1)
+        *reinterpret_cast<V2*>(row) = V2{v[r][0], v[r][1]};
+      else {
+        if (vx0) row[0] = v[r][0];
+        if (vx1) row[1] = v[r][1];
+      }
     }
   }
 }

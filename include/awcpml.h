@@ -191,9 +191,11 @@ int64_t awc_batch_step(const awc_batch* batch);
 /* One shot's traces (nt x nrec) and current field (nx*ny), as doubles. */
 int awc_batch_traces(awc_batch* batch, int32_t shot, double* traces);
 int awc_batch_field(awc_batch* batch, int32_t shot, double* p);
-/* Tile height (4, 8, 16, 32 or 64 rows of 32 nodes; 4 warps per block, each
- * streaming tile_y/4 rows) and resident blocks per SM (1..32) of the
- * persistent step kernel; results do not depend on them. */
+/* Tile height and resident blocks per SM (1..32) of the persistent step
+ * kernel; results do not depend on them. tile_y 4, 8 or 16: tiles 64 nodes
+ * wide staged through shared memory by TMA (4 consumer warps of tile_y/4 rows
+ * and a producer warp per block); 32 or 64: tiles 32 nodes wide read into
+ * registers (4 warps per block, each streaming tile_y/4 rows). */
 int awc_batch_set_launch(awc_batch* batch, int32_t tile_y, int32_t blocks_per_sm);
 int awc_batch_get_launch(const awc_batch* batch, int32_t* tile_y, int32_t* blocks_per_sm);
 /* Times every launch shape on the batch's data, keeps the fastest, resets. */
