@@ -1042,8 +1042,14 @@ __global__ void __launch_bounds__(32 * (BATCH_CW + 1))
   for (int u = 0; u < nu; ++u) {
     const int s = u % S;
     if (!mbar_wait(&full[s], (u / S) & 1, abort)) {
+      // a wait ran out: record it, stop, and let the loads that may still be
+      // in flight (at most S uses from here) land before the block ends
       *abort = 1;
       atomicExch(err, 1);
+      if (ct == 0)
+        for (int v = u; v < nu && v < u + S; ++v)
+          for (int n = 0; n < 64; ++n)
+            if (mbar_try_wait(&full[v % S], (v / S) & 1, 1000000u)) break;
       return;
     }
     const unsigned char* st = smem + s * L::BYTES;

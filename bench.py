@@ -270,9 +270,11 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "per_launch": "one time step of every shot of the rank's batch = one "
-                                       "persistent step2d_batch launch; A_eff summed over "
+                                       "persistent batched-step launch; A_eff summed over "
                                        "shots, FP32 words"},
-            "launch": {"tile": [32, ty], "blocks_per_sm": bps},
+            "launch": {"tile": [64 if ty <= 16 else 32, ty], "blocks_per_sm": bps,
+                       "kernel": "step2d_batch_tma (TMA stages, producer warp)" if ty <= 16
+                                 else "step2d_batch (register strips)"},
             "gpu_launches": k * nt, "timed_runs": k,
             "sharding": f"shots {rank}::{world} per rank" if world > 1 else "one batch"}
 
