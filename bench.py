@@ -48,6 +48,9 @@ def parse_args():
                     help="device-resident leg only (no e2e, FP64 or CPU legs); for profiling")
     ap.add_argument("--launch", default=None,
                     help="tile_y,zchunk,band_zchunk of the 3D step instead of autotuning")
+    ap.add_argument("--batch-only", default=None, metavar="TILE_Y,BLOCKS_PER_SM",
+                    help="profiling: only the batched 2D workload at --nt steps and this launch "
+                         "shape (one eager run, no timing line)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the CPU-baseline sample")
     return ap.parse_args()
@@ -279,6 +282,22 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak):
             "sharding": f"shots {rank}::{world} per rank" if world > 1 else "one batch"}
 
 
+def batch_profile_run(args, local):
+    """--batch-only: the batched 2D workload at args.nt steps with a fixed
+    launch shape, run once eagerly (one launch per step), for ncu."""
+    import __graft_entry__ as G
+    from acousticwavecpml_b200 import workloads as W
+    pkg = G.load_package()
+    w = W.config3(nt=args.nt)
+    probs, vels, setups, idx = pkg.prepare_batch(w["models"], W.batch_shots(pkg, w), **w["kwargs"])
+    b = pkg.Batch(pkg.Context(local), probs, vels, setups, idx)
+    ty, bps = (int(x) for x in args.batch_only.split(","))
+    b.set_launch(ty, bps)
+    b.run(args.nt, graph=False)
+    print(json.dumps({"batch_only": w["name"], "launch": [ty, bps], "steps": b.step}))
+    b.close()
+
+
 def gradient_leg(pkg, ctx, rank, world, timed_host):
     """3D gradient, FP32 with an FP64 check: one shot of the 16-shot
     gradient workload per rank (shot = rank), dJ/d(c²) at the initial model
@@ -350,6 +369,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
 
+    if args.batch_only:
+        batch_profile_run(args, local)
+        return
     pkg, w, srcs, recs = workload(args)
     s = pkg.prepare(w["lengths"], w["lt"], w["vel"], srcs, recs, precision=args.precision,
                     **w["kwargs"])
