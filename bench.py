@@ -285,9 +285,8 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak):
 def batch_profile_run(args, local):
     """--batch-only: the batched 2D workload at args.nt steps with a fixed
     launch shape, run once eagerly (one launch per step), for ncu."""
-    import __graft_entry__ as G
-    from acousticwavecpml_b200 import workloads as W
     pkg = G.load_package()
+    from acousticwavecpml_b200 import workloads as W
     w = W.config3(nt=args.nt)
     probs, vels, setups, idx = pkg.prepare_batch(w["models"], W.batch_shots(pkg, w), **w["kwargs"])
     b = pkg.Batch(pkg.Context(local), probs, vels, setups, idx)
