@@ -126,11 +126,31 @@ __device__ __forceinline__ T adj_band_terms(const AdjParams<T>& A, int a, int c,
   return r;
 }
 
-// λ_{t+1} without the receiver residuals: 2 λ_{t+2} - λ_{t+3} plus the
-// transposed stencil of G = F λ_{t+2} and the band terms; one thread per
-// node.
+// The residuals of step t enter λ_{t+1} = R_t + 2 λ_{t+2} - λ_{t+3} + ...
+// through λ_{t+3}: before adj_lambda_grad runs, λ_{t+3} -= R_t at the receiver
+// nodes (one thread per node, its receivers in receiver order), so that the
+// fused kernel needs no receiver lookup.
 template <typename T>
-__global__ void __launch_bounds__(256) adj_lambda(AdjParams<T> A) {
+__global__ void adj_residuals(T* __restrict__ lam3, const int64_t* __restrict__ node,
+                              const int32_t* __restrict__ off, const int32_t* __restrict__ ids,
+                              int32_t nnode, const T* __restrict__ res_row) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nnode) return;
+  T v = lam3[node[n]];
+  for (int e = off[n]; e < off[n + 1]; ++e) v -= res_row[ids[e]];
+  lam3[node[n]] = v;
+}
+
+// λ_{t+1} = 2 λ_{t+2} - λ_{t+3} (residuals included, see adj_residuals) plus
+// the transposed stencil of G = F λ_{t+2} and the band terms, one thread per
+// node; then at the same node G = F λ_{t+1} for the next step and the gradient accumulation dJ/dF += λ_{t+1} (p_{t+1} - 2 p_t +
+// p_{t-1}) / F (the source term is removed by adj_sources).
+template <typename T>
+__global__ void __launch_bounds__(256) adj_lambda_grad(AdjParams<T> A, T* __restrict__ Gn,
+                                                       const T* __restrict__ pm1,
+                                                       const T* __restrict__ p0,
+                                                       const T* __restrict__ pp1,
+                                                       double* __restrict__ grad) {
   const int i = 1 + blockIdx.x * 32 + threadIdx.x;
   const int j = 1 + blockIdx.y * 8 + threadIdx.y;
   const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
@@ -148,54 +168,38 @@ __global__ void __launch_bounds__(256) adj_lambda(AdjParams<T> A) {
     if (adj_band_near(A, k, A.nz)) lam += adj_band_terms(A, 2, k, A.nz, i, j, k);
   }
   A.lamn[o] = lam;
-}
-
-// λ_{t+1} += the residuals of step t at the receiver nodes (one thread per
-// node, its receivers summed in receiver order).
-template <typename T>
-__global__ void adj_residuals(T* __restrict__ lamn, const int64_t* __restrict__ node,
-                              const int32_t* __restrict__ off, const int32_t* __restrict__ ids,
-                              int32_t nnode, const T* __restrict__ res_row) {
-  const int n = blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= nnode) return;
-  T v = lamn[node[n]];
-  for (int e = off[n]; e < off[n + 1]; ++e) v += res_row[ids[e]];
-  lamn[node[n]] = v;
-}
-
-// G = F λ_{t+1} for the next step, and the gradient accumulation
-// dJ/dF += λ_{t+1} (p_{t+1} - 2 p_t + p_{t-1}) / F (the source term is
-// removed by adj_sources).
-template <typename T>
-__global__ void __launch_bounds__(256) adj_grad(AdjParams<T> A, T* __restrict__ Gn,
-                                                const T* __restrict__ pm1,
-                                                const T* __restrict__ p0,
-                                                const T* __restrict__ pp1,
-                                                double* __restrict__ grad) {
-  const int i = 1 + blockIdx.x * 32 + threadIdx.x;
-  const int j = 1 + blockIdx.y * 8 + threadIdx.y;
-  const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
-  if (i > A.nx - 2 || j > A.ny - 2) return;
-  const int64_t o = i + A.px * j + A.plane * k;
-  const T lam = A.lamn[o], f = A.F[o];
+  const T f = __ldg(A.F + o);
   Gn[o] = f * lam;
   if (grad) {
-    const double b = ((double)pp1[o] - 2.0 * (double)p0[o] + (double)pm1[o]) / (double)f;
+    const double b = ((double)__ldg(pp1 + o) - 2.0 * (double)__ldg(p0 + o) +
+                      (double)__ldg(pm1 + o)) / (double)f;
     grad[o] += (double)lam * b;
   }
 }
 
-// ν_{t+1} and μ_{t+1} of one axis side, one thread per band node (entry q,
-// other coordinates): ν_{t+1}[q-1] = bK ν_{t+2}[q-1] + F λ_{t+1}; face q
-// (and face 0 for q = 1) of μ in place, with w of node q+1 formed from
-// ν_{t+2} so that no thread reads another's new ν.
+// The active band sides of one adjoint step, for one launch over all of
+// them: side n is axis ax[n], side sd[n], band nodes [start[n], start[n+1]).
+struct AdjSides {
+  int32_t n;
+  int32_t ax[6], sd[6];
+  int64_t start[7];
+};
+
+// ν_{t+1} and μ_{t+1} of every active side, one thread per band node (side,
+// entry q, other coordinates): ν_{t+1}[q-1] = bK ν_{t+2}[q-1] + F λ_{t+1};
+// face q (and face 0 for q = 1) of μ in place, with w of node q+1 formed from
+// ν_{t+2} so that no thread reads another's new ν. Sides touch disjoint
+// arrays.
 template <typename T>
-__global__ void __launch_bounds__(256) adj_band(AdjParams<T> A, int a, int s, int64_t count) {
+__global__ void __launch_bounds__(256) adj_band(AdjParams<T> A, AdjSides L) {
   const int h = A.halo;
-  const int n1 = a == 0 ? A.ny - 2 : A.nx - 2;        // fastest other coordinate count
-  const int n2 = a == 2 ? A.ny - 2 : (A.ndim == 3 ? A.nz - 2 : 1);
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count;
-       t += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < L.start[L.n];
+       g += (int64_t)gridDim.x * blockDim.x) {
+    int side = 0;
+    while (side + 1 < L.n && g >= L.start[side + 1]) ++side;
+    const int a = L.ax[side], s = L.sd[side];
+    const int64_t t = g - L.start[side];
+    const int n1 = a == 0 ? A.ny - 2 : A.nx - 2;  // fastest other coordinate count
     int q, u, v;
     if (a == 0) {  // q fastest: ψ_x is contiguous in q
       q = 1 + (int)(t % h);
@@ -206,7 +210,6 @@ __global__ void __launch_bounds__(256) adj_band(AdjParams<T> A, int a, int s, in
       q = 1 + (int)((t / n1) % h);
       v = (int)(t / ((int64_t)n1 * h));
     }
-    (void)n2;
     const int c = q + A.off[a][s];
     int i, j, k;
     if (a == 0) { i = c; j = 1 + u; k = A.ndim == 3 ? 1 + v : 0; }
@@ -430,6 +433,22 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       A.mu[a][s] = mu[a][s];
     }
   }
+  // the active band sides, one launch per step over all of them
+  awc::AdjSides sides{};
+  sides.start[0] = 0;
+  for (int a = 0; a < p->ndim && h > 0; ++a)
+    for (int sd = 0; sd < 2; ++sd) {
+      if (!A.active[a][sd]) continue;
+      const int64_t n1 = a == 0 ? p->ny - 2 : p->nx - 2;
+      const int64_t n2 = p->ndim == 3 ? (a == 2 ? p->ny - 2 : V.nz - 2) : 1;
+      sides.ax[sides.n] = a;
+      sides.sd[sides.n] = sd;
+      sides.start[sides.n + 1] = sides.start[sides.n] + h * n1 * n2;
+      ++sides.n;
+    }
+  const unsigned band_blocks =
+      (unsigned)std::max<int64_t>(1, std::min<int64_t>((sides.start[sides.n] + 255) / 256,
+                                                       (int64_t)C->num_sms * 8));
   const dim3 blk(32, 8);
   const dim3 grid((unsigned)((p->nx - 2 + 31) / 32), (unsigned)((p->ny - 2 + 7) / 8),
                   (unsigned)(p->ndim == 3 ? V.nz - 2 : 1));
@@ -508,7 +527,7 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       if (rc) return rc;
     }
     for (int64_t t = e - 1; t >= s; --t) {
-      // λ_{t+1} overwrites λ_{t+3}: adj_lambda reads λ_{t+3} only at the
+      // λ_{t+1} overwrites λ_{t+3}: adj_lambda_grad reads λ_{t+3} only at the
       // node it writes
       T* ln = lam[i3];
       A.lam2 = lam[i2];
@@ -520,26 +539,17 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
           A.nu_old[a][sd] = nu[a][sd][par];
           A.nu_new[a][sd] = nu[a][sd][par ^ 1];
         }
-      awc::adj_lambda<T><<<grid, blk, 0, st>>>(A);
       if (!RG.node.empty())
         awc::adj_residuals<T><<<(unsigned)((RG.node.size() + 127) / 128), 128, 0, st>>>(
             ln, rnode_d, roff_d, rids_d, (int32_t)RG.node.size(), res_d + t * nrec);
       const T* pm1 = want_grad ? seg[t - s] : nullptr;
       const T* p0 = want_grad ? seg[t - s + 1] : nullptr;
       const T* pp1 = want_grad ? seg[t - s + 2] : nullptr;
-      awc::adj_grad<T><<<grid, blk, 0, st>>>(A, G[gi ^ 1], pm1, p0, pp1, grad);
+      awc::adj_lambda_grad<T><<<grid, blk, 0, st>>>(A, G[gi ^ 1], pm1, p0, pp1, grad);
       if (nsrc > 0)
         awc::adj_sources<T><<<1, 32, 0, st>>>(ln, A.F, snode_d, (int32_t)nsrc, stf_d + t * nsrc,
                                               grad, sout_d ? sout_d + t * nsrc : nullptr);
-      for (int a = 0; a < p->ndim; ++a)
-        for (int sd = 0; sd < 2; ++sd) {
-          if (!A.active[a][sd] || h == 0) continue;
-          const int64_t n1 = a == 0 ? p->ny - 2 : p->nx - 2;
-          const int64_t n2 = p->ndim == 3 ? (a == 2 ? p->ny - 2 : V.nz - 2) : 1;
-          const int64_t count = h * n1 * n2;
-          const unsigned nb = (unsigned)std::min<int64_t>((count + 255) / 256, (int64_t)C->num_sms * 8);
-          awc::adj_band<T><<<nb, 256, 0, st>>>(A, a, sd, count);
-        }
+      if (sides.n > 0) awc::adj_band<T><<<band_blocks, 256, 0, st>>>(A, sides);
       ADJ_TRY(C, cudaGetLastError());
       std::swap(i2, i3);  // λ_{t+1} is the next step's λ_{t+2}
       par ^= 1;
