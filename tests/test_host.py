@@ -156,6 +156,23 @@ def test_a_eff_matches_reference_formula(pkg):
     assert abs(ref * 4 / 1e6 - 597.8) < 0.1  # MB per step in FP32
 
 
+def test_bench_min_traffic(pkg):
+    """The bench line's minimal traffic at 296 x 276 x 296 (halo 20, free
+    top): 4 field words per interior node plus a read and a write of every
+    live ψ (h + 1 layers) and ξ (h layers) entry, FP32."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    p = _problem(pkg, nx=296, ny=276, nz=296, halo=20, freetop=1)
+    cells = 294 * 274 * 294
+    band = 2 * 2 * 41 * (274 * 294) + 1 * 2 * 41 * (294 * 294) + 2 * 2 * 41 * (294 * 274)
+    assert bench.min_traffic(p) == 4 * (4 * cells + band) == 512975904
+    p.freetop = 0
+    band += 2 * 41 * (294 * 294)
+    assert bench.min_traffic(p) == 4 * (4 * cells + band)
+
+
 def test_create_without_device_fails_cleanly(pkg):
     import torch
     if torch.cuda.is_available():
