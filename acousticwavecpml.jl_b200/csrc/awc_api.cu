@@ -180,7 +180,6 @@ struct awc_plan {
   awc::IoRim* io_rim = nullptr;
   int32_t io_nrim = 0;
   uint64_t io_shape = ~0ull;  // launch shape io_* were built for
-  uint32_t io_version = 0;
   // 3D regions: the band-free core box and the shell boxes around it
   bool has_core = false;
   awc::Box core{};
@@ -203,7 +202,27 @@ struct awc_plan {
   int64_t step = 0;
   int32_t active[3][2] = {};
   std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
-  uint64_t graph_key = 0;  // launch configuration the graphs were captured with
+  // Everything the captured kernel parameters hold by value besides the grid
+  // shape and the fixed device buffers: the graphs are reused while it is
+  // unchanged (a new shot of the same shape re-uploads data only).
+  struct GraphKey {
+    uint64_t launch = ~0ull;
+    int32_t active[3][2] = {};
+    double d[3] = {};
+    int32_t nrim = -1, do_rim[2] = {};
+    const void* blk_off[2] = {};
+    bool operator==(const GraphKey& o) const {
+      if (launch != o.launch || nrim != o.nrim || do_rim[0] != o.do_rim[0] ||
+          do_rim[1] != o.do_rim[1] || blk_off[0] != o.blk_off[0] || blk_off[1] != o.blk_off[1])
+        return false;
+      for (int a = 0; a < 3; ++a) {
+        if (d[a] != o.d[a]) return false;
+        for (int s = 0; s < 2; ++s)
+          if (active[a][s] != o.active[a][s]) return false;
+      }
+      return true;
+    }
+  } graph_key;
   // copy of each new field to keep: after step it in [keep_first,
   // keep_first + keep_count) the new field goes to keep[it - keep_first]
   // (eager runs only; set by the adjoint's segment recompute)
@@ -666,7 +685,6 @@ int ensure_io(awc_plan* P) {
   CUDA_TRY(&C->err, cudaStreamSynchronize(st));
   P->io_nrim = (int32_t)rim.size();
   P->io_shape = launch_shape(P);
-  P->io_version++;
   return AWC_OK;
 }
 
@@ -797,17 +815,26 @@ int prepare_launch(awc_plan* P) {
   return AWC_OK;
 }
 
-uint64_t config_key(const awc_plan* P) {
-  uint64_t k = launch_shape(P) ^ ((uint64_t)(P->io_version & 0xffff) << 24);
+awc_plan::GraphKey config_key(const awc_plan* P) {
+  awc_plan::GraphKey k;
+  k.launch = launch_shape(P);
   for (int a = 0; a < 3; ++a)
-    for (int s = 0; s < 2; ++s) k ^= (uint64_t)P->active[a][s] << (48 + 2 * a + s);
+    for (int s = 0; s < 2; ++s) k.active[a][s] = P->active[a][s];
+  k.d[0] = P->p.dx;
+  k.d[1] = P->p.dy;
+  k.d[2] = P->p.ndim == 3 ? P->p.dz : 1.0;
+  k.nrim = P->io_nrim;
+  for (int w = 0; w < 2; ++w) {
+    k.do_rim[w] = P->io_k[w].do_rim;
+    k.blk_off[w] = P->io_k[w].blk_off;
+  }
   return k;
 }
 
 int get_graph(awc_plan* P, int64_t start, int64_t n, cudaGraphExec_t* out) {
   awc_ctx* C = P->ctx;
-  const uint64_t key = config_key(P);
-  if (key != P->graph_key) {
+  const awc_plan::GraphKey key = config_key(P);
+  if (!(key == P->graph_key)) {
     P->drop_graphs();
     P->graph_key = key;
   }
