@@ -18,7 +18,9 @@
 
 #include <cstdio>
 #include <cstring>
-#include <mutex>
+#include <algorithm>
+#include <cmath>
+#include <vector>
 
 #include "../../include/awcpml.h"
 #include "awc_kernels.cuh"
@@ -30,7 +32,6 @@ void record_error(const char* msg);  // awc_api.cu
 namespace {
 
 constexpr size_t kScratchBytes = size_t(32) << 20;  // 32 MiB
-constexpr int kMaxDevices = 64;
 
 // The scratch array. In host code this name is only a stand-in for the
 // device symbol: its device address comes from cudaGetSymbolAddress.
@@ -41,47 +42,49 @@ int fail(int code, const char* msg) {
   return code;
 }
 
-// Device address of g_scratch on the current device, looked up once per
-// device (the first call on each device does it).
+// Device address of g_scratch on the current device. It is looked up on
+// every call rather than cached: a cached address would dangle after a device
+// reset (cudaDeviceReset, CUDA.jl's device_reset!), which reloads the module.
+// The first lookup on a device loads the module there.
 int scratch_address(unsigned char** out) {
-  static std::mutex mu;
-  static unsigned char* addr[kMaxDevices] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+  if (e != cudaSuccess) {
     cudaGetLastError();
-    return fail(AWC_ERR_NODEVICE, "no current CUDA device");
+    return fail(e == cudaErrorNoDevice || e == cudaErrorInvalidDevice ? AWC_ERR_NODEVICE
+                                                                       : AWC_ERR_CUDA,
+                cudaGetErrorString(e));
   }
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      return fail(AWC_ERR_CUDA, cudaGetErrorString(e));
-    }
-    addr[dev] = static_cast<unsigned char*>(p);
-  }
-  *out = addr[dev];
+  *out = static_cast<unsigned char*>(p);
   return AWC_OK;
 }
 
 size_t up256(size_t b) { return (b + 255) / 256 * 256; }
 
-// Sources then receivers of step `it`, in one block: each source adds its
-// scaled time function to the new field at its node, then each receiver
-// samples the new field (reference inject_sources!/record_receivers!).
-__global__ void static_io(float* pnew, const double* dt2srctf, const int64_t* possrcs, int nsrc,
-                          const int64_t* posrecs, int nrec, int64_t nt, int64_t it, int64_t nx,
+// Sources then receivers of step `it`, in one block (reference
+// inject_sources!/record_receivers!). Sources are grouped by node on the
+// host; one thread owns a group and adds its sources in source order, so
+// several sources on one node are summed in the order awc_forward sums them.
+// Then each receiver samples the new field.
+__global__ void static_io(float* pnew, const double* stf, const int64_t* grp_node,
+                          const int32_t* grp_off, const int32_t* grp_src, int ngrp,
+                          const int64_t* rec_node, int nrec, int64_t nt, int64_t it,
                           double* traces) {
-  for (int s = threadIdx.x; s < nsrc; s += blockDim.x) {
-    const int64_t node = (possrcs[s] - 1) + nx * (possrcs[s + nsrc] - 1);
-    atomicAdd(pnew + node, (float)dt2srctf[it + nt * s]);
+  for (int g = threadIdx.x; g < ngrp; g += blockDim.x) {
+    float v = pnew[grp_node[g]];
+    for (int e = grp_off[g]; e < grp_off[g + 1]; ++e) v += (float)stf[it + nt * grp_src[e]];
+    pnew[grp_node[g]] = v;
   }
   __syncthreads();
-  for (int r = threadIdx.x; r < nrec; r += blockDim.x) {
-    const int64_t node = (posrecs[r] - 1) + nx * (posrecs[r + nrec] - 1);
-    traces[it + nt * r] = (double)pnew[node];
-  }
+  for (int r = threadIdx.x; r < nrec; r += blockDim.x)
+    traces[it + nt * r] = (double)pnew[rec_node[r]];
+}
+
+// a * b, or false when the product of two non-negative sizes overflows.
+bool mul_ok(size_t a, size_t b, size_t* out) {
+  if (a != 0 && b > SIZE_MAX / a) return false;
+  *out = a * b;
+  return true;
 }
 
 __global__ void static_narrow(const double* src, float* dst, int64_t n) {
@@ -113,10 +116,15 @@ extern "C" int awc_forward2d_f32_static(const awc_problem* p, const double* vel,
     return fail(AWC_ERR_INVALID, "grid size must be in [3, 2^20] per axis");
   if (p->halo < 0 || p->halo > p->nx - 2 || p->halo > p->ny - 2)
     return fail(AWC_ERR_INVALID, "halo out of range for the grid");
-  if (!(p->dx > 0.0) || !(p->dy > 0.0) || !(p->dt > 0.0))
-    return fail(AWC_ERR_INVALID, "grid spacing and dt must be positive");
-  if (p->nt < 0 || p->nsrc < 0 || p->nrec < 0 || p->nsrc > (1 << 20) || p->nrec > (1 << 20))
-    return fail(AWC_ERR_INVALID, "nt/nsrc/nrec out of range");
+  if (!(p->dx > 0.0) || !(p->dy > 0.0) || !(p->dt > 0.0) || !std::isfinite(p->dx) ||
+      !std::isfinite(p->dy) || !std::isfinite(p->dt))
+    return fail(AWC_ERR_INVALID, "grid spacing and dt must be positive and finite");
+  // the same limits as awc_forward: nt <= 2^31, so step indices fit in int32
+  // and every size below fits in size_t without overflow
+  if (p->nt < 0 || p->nt > ((int64_t)1 << 31))
+    return fail(AWC_ERR_INVALID, "nt out of range");
+  if (p->nsrc < 0 || p->nrec < 0 || p->nsrc > (1 << 20) || p->nrec > (1 << 20))
+    return fail(AWC_ERR_INVALID, "nsrc/nrec out of range");
   if (!vel || !coeffs || (p->nsrc > 0 && (!possrcs || (p->nt > 0 && !dt2srctf))) ||
       (p->nrec > 0 && !posrecs) || (p->nt * p->nrec > 0 && !traces))
     return fail(AWC_ERR_INVALID, "a required array is NULL");
@@ -128,36 +136,73 @@ extern "C" int awc_forward2d_f32_static(const awc_problem* p, const double* vel,
     if (posrecs[r] < 1 || posrecs[r] > nx || posrecs[r + nr] < 1 || posrecs[r + nr] > ny)
       return fail(AWC_ERR_INVALID, "At least one receiver is not inside the model!");
 
+  // sources grouped by node, in source order within a group
+  std::vector<int32_t> order((size_t)ns);
+  for (int64_t s = 0; s < ns; ++s) order[s] = (int32_t)s;
+  auto src_node = [&](int64_t s) { return (possrcs[s] - 1) + nx * (possrcs[s + ns] - 1); };
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int32_t a, int32_t b) { return src_node(a) < src_node(b); });
+  std::vector<int64_t> grp_node, rec_node((size_t)nr);
+  std::vector<int32_t> grp_off;
+  for (int64_t e = 0; e < ns; ++e) {
+    if (e == 0 || src_node(order[e]) != src_node(order[e - 1])) {
+      grp_node.push_back(src_node(order[e]));
+      grp_off.push_back((int32_t)e);
+    }
+  }
+  grp_off.push_back((int32_t)ns);
+  for (int64_t r = 0; r < nr; ++r) rec_node[r] = (posrecs[r] - 1) + nx * (posrecs[r + nr] - 1);
+  const int64_t ngrp = (int64_t)grp_node.size();
+
   // ---- scratch layout (every region 256-byte aligned) --------------------
+  // With the limits above every product fits in size_t; the sizes are still
+  // formed with checked multiplies so that no wrapped size can pass the
+  // capacity test.
   const int64_t N = nx * ny;
   const int gx = (int)((nx - 2) / 32 + 1), gy = (int)((ny - 2 + 7) / 8);
   const int64_t clen = 2 * (8 * h + 4);
   size_t off = 0;
-  auto take = [&](size_t bytes) {
+  bool fits = true;
+  auto take = [&](size_t count, size_t elem) {
+    size_t bytes = 0;
     const size_t at = off;
+    if (!mul_ok(count, elem, &bytes) || bytes > kScratchBytes) {
+      fits = false;
+      return at;
+    }
     off += up256(bytes);
     return at;
   };
-  const size_t o_buf = take(3 * N * sizeof(float));
-  const size_t o_fact = take(N * sizeof(float));
-  const size_t o_vel = take(N * sizeof(double));  // vel in, then pfinal out
-  const size_t o_psx = take(2 * 2 * (h + 1) * ny * sizeof(float));
-  const size_t o_xix = take(2 * h * ny * sizeof(float));
-  const size_t o_psy = take(2 * 2 * (h + 1) * nx * sizeof(float));
-  const size_t o_xiy = take(2 * h * nx * sizeof(float));
-  const size_t o_cd = take(clen * sizeof(double));
-  const size_t o_cf = take(clen * sizeof(float));
-  const size_t o_stf = take(nt * ns * sizeof(double));
-  const size_t o_ps = take(2 * ns * sizeof(int64_t));
-  const size_t o_pr = take(2 * nr * sizeof(int64_t));
-  const size_t o_tr = take(nt * nr * sizeof(double));
-  const size_t o_blk = take(((int64_t)gx * gy + 1) * sizeof(int32_t));
-  if (off > kScratchBytes) {
+  size_t nt_ns = 0, nt_nr = 0;
+  fits = mul_ok((size_t)nt, (size_t)ns, &nt_ns) && mul_ok((size_t)nt, (size_t)nr, &nt_nr);
+  const size_t o_buf = take(3 * (size_t)N, sizeof(float));
+  const size_t o_fact = take((size_t)N, sizeof(float));
+  const size_t o_vel = take((size_t)N, sizeof(double));  // vel in, then pfinal out
+  const size_t o_psx = take(2 * 2 * (size_t)(h + 1) * ny, sizeof(float));
+  const size_t o_xix = take(2 * (size_t)h * ny, sizeof(float));
+  const size_t o_psy = take(2 * 2 * (size_t)(h + 1) * nx, sizeof(float));
+  const size_t o_xiy = take(2 * (size_t)h * nx, sizeof(float));
+  const size_t o_cd = take((size_t)clen, sizeof(double));
+  const size_t o_cf = take((size_t)clen, sizeof(float));
+  const size_t o_stf = take(nt_ns, sizeof(double));
+  const size_t o_gn = take((size_t)ngrp, sizeof(int64_t));
+  const size_t o_go = take((size_t)ngrp + 1, sizeof(int32_t));
+  const size_t o_gs = take((size_t)ns, sizeof(int32_t));
+  const size_t o_pr = take((size_t)nr, sizeof(int64_t));
+  const size_t o_tr = take(nt_nr, sizeof(double));
+  const size_t o_blk = take((size_t)gx * gy + 1, sizeof(int32_t));
+  if (!fits || off > kScratchBytes) {
     char msg[200];
-    std::snprintf(msg, sizeof msg,
-                  "problem needs %zu bytes of device scratch; this entry point has %zu "
-                  "(use awc_forward for larger problems)",
-                  off, kScratchBytes);
+    if (fits)
+      std::snprintf(msg, sizeof msg,
+                    "problem needs %zu bytes of device scratch; this entry point has %zu "
+                    "(use awc_forward for larger problems)",
+                    off, kScratchBytes);
+    else
+      std::snprintf(msg, sizeof msg,
+                    "problem needs more than the %zu bytes of device scratch this entry point "
+                    "has (use awc_forward for larger problems)",
+                    kScratchBytes);
     return fail(AWC_ERR_INVALID, msg);
   }
 
@@ -177,8 +222,12 @@ extern "C" int awc_forward2d_f32_static(const awc_problem* p, const double* vel,
   STATIC_TRY(cudaMemcpy(S + o_cd, coeffs, clen * sizeof(double), cudaMemcpyHostToDevice));
   if (nt * ns > 0)
     STATIC_TRY(cudaMemcpy(S + o_stf, dt2srctf, nt * ns * sizeof(double), cudaMemcpyHostToDevice));
-  if (ns > 0) STATIC_TRY(cudaMemcpy(S + o_ps, possrcs, 2 * ns * sizeof(int64_t), cudaMemcpyHostToDevice));
-  if (nr > 0) STATIC_TRY(cudaMemcpy(S + o_pr, posrecs, 2 * nr * sizeof(int64_t), cudaMemcpyHostToDevice));
+  if (ns > 0) {
+    STATIC_TRY(cudaMemcpy(S + o_gn, grp_node.data(), ngrp * sizeof(int64_t), cudaMemcpyHostToDevice));
+    STATIC_TRY(cudaMemcpy(S + o_go, grp_off.data(), (ngrp + 1) * sizeof(int32_t), cudaMemcpyHostToDevice));
+    STATIC_TRY(cudaMemcpy(S + o_gs, order.data(), ns * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
+  if (nr > 0) STATIC_TRY(cudaMemcpy(S + o_pr, rec_node.data(), nr * sizeof(int64_t), cudaMemcpyHostToDevice));
   awc::make_fact<float><<<256, 256>>>(veld, fact, p->dt * p->dt, N, nx, nx);
   static_narrow<<<1, 256>>>((const double*)(S + o_cd), cf, clen);
   STATIC_TRY(cudaGetLastError());
@@ -233,10 +282,12 @@ extern "C" int awc_forward2d_f32_static(const awc_problem* p, const double* vel,
 
   // ---- time loop ----------------------------------------------------------
   const double* stf = (const double*)(S + o_stf);
-  const int64_t* dps = (const int64_t*)(S + o_ps);
-  const int64_t* dpr = (const int64_t*)(S + o_pr);
+  const int64_t* gnode = (const int64_t*)(S + o_gn);
+  const int32_t* goff = (const int32_t*)(S + o_go);
+  const int32_t* gsrc = (const int32_t*)(S + o_gs);
+  const int64_t* rnode = (const int64_t*)(S + o_pr);
   double* dtr = (double*)(S + o_tr);
-  const int io_threads = (int)((ns > nr ? ns : nr) > 255 ? 256 : 32);
+  const int io_threads = (int)((ngrp > nr ? ngrp : nr) > 255 ? 256 : 32);
   for (int64_t it = 0; it < nt; ++it) {
     P.pold = buf[it % 3];
     P.pcur = buf[(it + 1) % 3];
@@ -250,7 +301,8 @@ extern "C" int awc_forward2d_f32_static(const awc_problem* p, const double* vel,
     P.it = (int32_t)it;
     awc::step2d<float><<<dim3(gx, gy), dim3(32, 8)>>>(P);
     if (ns > 0 || nr > 0)
-      static_io<<<1, io_threads>>>(P.pnew, stf, dps, (int)ns, dpr, (int)nr, nt, it, nx, dtr);
+      static_io<<<1, io_threads>>>(P.pnew, stf, gnode, goff, gsrc, (int)ngrp, rnode, (int)nr, nt,
+                                   it, dtr);
   }
   STATIC_TRY(cudaGetLastError());
 

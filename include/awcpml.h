@@ -263,8 +263,12 @@ int awc_forward_learned(awc_ctx* ctx, const awc_problem* p, const double* vel,
  * about 24 nx ny + 8 nt nrec + 8 nt nsrc bytes plus the CPML band arrays;
  * larger problems are rejected with AWC_ERR_INVALID and a message giving the
  * size needed (use awc_forward for them).
- * The first call on each device looks up the array's device address; make
- * that first call before any stream capture. Every call clears the state it
+ * Every call looks up the array's device address with cudaGetSymbolAddress
+ * (so a device reset between calls is harmless); the first call on a device
+ * also loads the module there, so make that first call before any stream
+ * capture. Several sources on one node are summed in source order, as in
+ * awc_forward, and the scalar limits are awc_forward's (nt <= 2^31, finite
+ * positive spacing and dt). Every call clears the state it
  * needs, but all calls share the one array: calls that overlap on the GPU
  * (from several host threads on one device) race and must be serialised by
  * the caller. Runs on the current device and the legacy default stream and

@@ -72,3 +72,33 @@ def test_static_rejects_oversized_and_unsupported_problems(pkg):
                       **w["kwargs"])
     rc, _, _ = _static(pkg, s64)
     assert rc == pkg._lib.AWC_ERR_INVALID
+
+
+def test_static_rejects_bad_scalars_before_any_device_work(pkg):
+    """nt beyond 2^31 (whose trace and source sizes would wrap a 64-bit byte
+    count near 2^41), non-finite spacing or dt, and NULL arrays are refused on
+    the host with AWC_ERR_INVALID, the limits awc_forward applies; no device
+    memory is touched, so this runs without a GPU."""
+    from acousticwavecpml_b200 import workloads as W
+    w = W.config1()
+    srcs, recs = W.sources_receivers(pkg, w)
+    s = pkg.prepare(w["lengths"], w["lt"], w["vel"], srcs, recs, precision="f32", **w["kwargs"])
+    p = s["problem"]
+    lib = pkg._lib.lib()
+    for field, value in (("nt", (1 << 41) + 3), ("nt", (1 << 31) + 1), ("nt", -1),
+                         ("dx", float("inf")), ("dy", float("nan")), ("dt", float("inf")),
+                         ("dt", 0.0)):
+        bad = pkg._lib.Problem.from_buffer_copy(p)
+        setattr(bad, field, value)
+        rc = lib.awc_forward2d_f32_static(
+            ctypes.byref(bad), s["vel"].ctypes.data, s["coeffs"].ctypes.data,
+            s["possrcs"].ctypes.data, s["dt2srctf"].ctypes.data, s["posrecs"].ctypes.data,
+            None, None)
+        assert rc == pkg._lib.AWC_ERR_INVALID, (field, value)
+        msg = lib.awc_last_error(None)
+        assert (b"nt out of range" in msg) if field == "nt" else (b"positive and finite" in msg)
+    rc = lib.awc_forward2d_f32_static(ctypes.byref(p), None, s["coeffs"].ctypes.data,
+                                      s["possrcs"].ctypes.data, s["dt2srctf"].ctypes.data,
+                                      s["posrecs"].ctypes.data, None, None)
+    assert rc == pkg._lib.AWC_ERR_INVALID
+    assert b"NULL" in lib.awc_last_error(None)
