@@ -144,6 +144,30 @@ class Plan:
                                              ctypes.byref(bz)), self.ctx.handle)
         return ty.value, zc.value, bz.value
 
+    def set_blocking(self, depth, zchunks=2):
+        """Time steps per kernel pass (1 or 2) and z chunks per column tile of
+        the two-step kernel; results do not depend on either."""
+        check(_lib.lib().awc_plan_set_blocking(self._h, int(depth), int(zchunks)),
+              self.ctx.handle)
+
+    def get_blocking(self):
+        d, z = ctypes.c_int32(), ctypes.c_int32()
+        check(_lib.lib().awc_plan_get_blocking(self._h, ctypes.byref(d), ctypes.byref(z)),
+              self.ctx.handle)
+        return d.value, z.value
+
+    def launch_count(self, nsteps=None):
+        """Kernel launches a run of nsteps (default: the remaining steps) issues."""
+        if nsteps is None:
+            nsteps = self.problem.nt
+        return int(_lib.lib().awc_plan_launch_count(self._h, int(nsteps)))
+
+    def set_wait(self, rounds=4096, round_ns=1000000, withhold=-1):
+        """Bounded-wait budget of the two-step kernel's pipeline; `withhold`
+        (tests of the timeout path only) makes every block skip one load."""
+        check(_lib.lib().awc_plan_set_wait(self._h, int(rounds), int(round_ns), int(withhold)),
+              self.ctx.handle)
+
     def autotune(self, steps=20):
         """Picks the fastest launch shape on this plan's data; resets the state.
         Returns the best time per step in ms."""

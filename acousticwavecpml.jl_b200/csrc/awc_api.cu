@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -25,6 +26,7 @@
 #include "../../include/awcpml.h"
 #include "awc_ctx.h"
 #include "awc_kernels.cuh"
+#include "awc_tb.cuh"
 
 namespace {
 
@@ -147,6 +149,41 @@ int64_t node_of(const awc_problem* p, int64_t px, const int64_t* pos, int64_t cn
 template <typename T>
 constexpr int stages() { return 5; }
 
+// Where the fields and the CPML state of the current step live. ord[0] is
+// the buffer of the newest pressure field p_s, ord[1] of p_{s-1}, ord[2] of
+// p_{s-2}, ord[3] the fourth buffer (3D plans). A one-step launch reads
+// ord[1], ord[0] and writes ord[2] (the reference's three-buffer rotation,
+// forward! at acoustic_3D_xPU.jl:166, which sources on the Dirichlet rim rely
+// on); a two-step pass reads ord[1], ord[0] and writes ord[2], ord[3]. ψ_s is
+// psi[..][psi_par]; ξ_s is xi (xi_par 0) or xi_alt (1).
+struct StepState {
+  int8_t ord[4] = {1, 0, 2, 3};
+  int8_t psi_par = 0, xi_par = 0;
+  void step1() {
+    const int8_t o[4] = {ord[2], ord[0], ord[1], ord[3]};
+    std::memcpy(ord, o, 4);
+    psi_par ^= 1;
+  }
+  void pass2() {
+    const int8_t o[4] = {ord[3], ord[2], ord[0], ord[1]};
+    std::memcpy(ord, o, 4);
+    psi_par ^= 1;
+    xi_par ^= 1;
+  }
+  // the state after `it` one-step launches from the initial one
+  static StepState after_steps(int64_t it) {
+    StepState s;
+    s.ord[0] = (int8_t)((it + 1) % 3);
+    s.ord[1] = (int8_t)(it % 3);
+    s.ord[2] = (int8_t)((it + 2) % 3);
+    s.psi_par = (int8_t)(it & 1);
+    return s;
+  }
+  int code() const {
+    return ord[0] | ord[1] << 2 | ord[2] << 4 | ord[3] << 6 | psi_par << 8 | xi_par << 9;
+  }
+};
+
 }  // namespace
 
 struct awc_plan {
@@ -158,10 +195,12 @@ struct awc_plan {
   int64_t NP = 0;  // pitched field length
   int64_t psi_side[3] = {}, xi_side[3] = {};  // right side's ψ / ξ offset from the left's (elements)
   // device buffers
-  void* buf[3] = {nullptr, nullptr, nullptr};
+  void* buf[4] = {nullptr, nullptr, nullptr, nullptr};  // 4th: 3D plans only
+  int32_t nbuf = 3;
   void* fact = nullptr;
   void* psi[3][2][2] = {};  // [axis][side][old/new parity]
   void* xi[3][2] = {};
+  void* xi_alt[3][2] = {};  // 3D: the second ξ array of two-step passes
   void* coef = nullptr;  // packed coefficients in T
   int32_t* err_flag = nullptr;
   // sources and receivers: groups per node (CSR), the nodes themselves, and
@@ -175,6 +214,7 @@ struct awc_plan {
     int32_t* blk_off = nullptr;
     int64_t cap = 0;
     int4* ent = nullptr;
+    int64_t ecap = 0;
     int32_t do_rim = 0;
   } io_k[2];                         // [0] 3D core or 2D kernel, [1] 3D shell kernel
   awc::IoRim* io_rim = nullptr;
@@ -196,12 +236,26 @@ struct awc_plan {
   // launch shape of the 3D core kernel: tile rows (4, 8, 16; the tile is
   // 64 x by nodes, 32 x by/2 threads) and z planes per block
   int32_t by = 8, zchunk = 1;
-  CUtensorMap map_c[3], map_o[3], map_f;
+  CUtensorMap map_c[4], map_o[4], map_f;
   int32_t maps_by = 0;  // tile height the tensor maps were encoded for
+  // two-step passes (awc_tb.cuh): depth 2 advances two steps per pass
+  int32_t depth = 1;
+  int32_t tb_nch = 1;        // z chunks per column tile
+  int32_t tb_zc = 1;         // planes per chunk
+  int32_t tb_ntiles[2] = {};  // [0] Z tiles, [1] XY tiles
+  int2* tb_tiles[2] = {};
+  int64_t tb_tiles_cap[2] = {};
+  IoSet tb_io[2];
+  uint64_t tb_io_shape = ~0ull;
+  CUtensorMap tb_map_pt[4], tb_map_in[4], tb_map_f;
+  bool tb_maps = false;
+  int32_t wait_rounds = 4096, wait_ns = 1000000, withhold = -1;
   // run state
   int64_t step = 0;
+  StepState state;
   int32_t active[3][2] = {};
-  std::map<std::pair<int64_t, int64_t>, cudaGraphExec_t> graphs;
+  // captured runs, by (first step, steps, state code at the first step)
+  std::map<std::array<int64_t, 3>, cudaGraphExec_t> graphs;
   // Everything the captured kernel parameters hold by value besides the grid
   // shape and the fixed device buffers: the graphs are reused while it is
   // unchanged (a new shot of the same shape re-uploads data only).
@@ -210,11 +264,19 @@ struct awc_plan {
     int32_t active[3][2] = {};
     double d[3] = {};
     int32_t nrim = -1, do_rim[2] = {};
-    const void* blk_off[2] = {};
+    const void* blk_off[4] = {};  // one-step core/shell, two-step Z/XY
+    const void* tiles[2] = {};
+    int32_t wait[3] = {};
     bool operator==(const GraphKey& o) const {
       if (launch != o.launch || nrim != o.nrim || do_rim[0] != o.do_rim[0] ||
-          do_rim[1] != o.do_rim[1] || blk_off[0] != o.blk_off[0] || blk_off[1] != o.blk_off[1])
+          do_rim[1] != o.do_rim[1])
         return false;
+      for (int w = 0; w < 4; ++w)
+        if (blk_off[w] != o.blk_off[w]) return false;
+      for (int w = 0; w < 2; ++w)
+        if (tiles[w] != o.tiles[w]) return false;
+      for (int w = 0; w < 3; ++w)
+        if (wait[w] != o.wait[w]) return false;
       for (int a = 0; a < 3; ++a) {
         if (d[a] != o.d[a]) return false;
         for (int s = 0; s < 2; ++s)
@@ -281,7 +343,8 @@ int plan_alloc(awc_plan* P) {
   P->px = pitch_of(p->nx);
   P->NP = P->px * p->ny * nz;
   int rc;
-  for (int b = 0; b < 3; ++b)
+  P->nbuf = p->ndim == 3 ? 4 : 3;
+  for (int b = 0; b < P->nbuf; ++b)
     if ((rc = P->alloc(&P->buf[b], P->NP * P->esz))) return rc;
   if ((rc = P->alloc(&P->fact, P->NP * P->esz))) return rc;
   // ψ (each parity) and ξ of an axis: one allocation per array kind, the
@@ -301,6 +364,11 @@ int plan_alloc(awc_plan* P) {
     if ((rc = P->alloc(&base, 2 * P->xi_side[a] * P->esz))) return rc;
     P->xi[a][0] = base;
     P->xi[a][1] = (char*)base + P->xi_side[a] * P->esz;
+    if (p->ndim == 3) {
+      if ((rc = P->alloc(&base, 2 * P->xi_side[a] * P->esz))) return rc;
+      P->xi_alt[a][0] = base;
+      P->xi_alt[a][1] = (char*)base + P->xi_side[a] * P->esz;
+    }
   }
   if ((rc = P->alloc(&P->coef, awc_coeffs_len(p) * P->esz))) return rc;
   if ((rc = P->alloc((void**)&P->err_flag, 4))) return rc;
@@ -334,6 +402,7 @@ int grid_for(const awc_ctx* C, int64_t n, int threads) {
 
 void make_regions(awc_plan* P);
 void box_blocks(awc_plan* P);
+bool tb_eligible(const awc_plan* P);
 
 // Uploads the inputs of one shot into an allocated plan. The copies are
 // stream-ordered on the context stream.
@@ -379,6 +448,7 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
     }
   }
   if (p->ndim == 3) make_regions(P);
+  P->tb_io_shape = ~0ull;
   // every node carrying sources and/or receivers, in first-appearance order
   // (sources first); its sources are summed in source order
   {
@@ -429,6 +499,7 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
     if (!rids.empty())
       CUDA_TRY(err, cudaMemcpyAsync(P->rec_ids, rids.data(), rids.size() * 4, cudaMemcpyHostToDevice, st));
     P->io_shape = ~0ull;  // rebuild the block lists before the next launch
+    P->tb_io_shape = ~0ull;
     // stf rows: [it][s] from the column-major (nt x nsrc) input
     std::vector<double> rows((size_t)std::max<int64_t>(nt * nsrc, 1), 0.0);
     for (int64_t s = 0; s < nsrc; ++s)
@@ -438,22 +509,22 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
       CUDA_TRY(err, cudaMemcpyAsync(P->stf, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, st));
     CUDA_TRY(err, cudaStreamSynchronize(st));  // host vectors go out of scope
   }
+  if (P->depth == 2 && !tb_eligible(P)) P->depth = 1;  // this shot has rim sources/receivers
   return AWC_OK;
 }
 
 // Parameters of step `it` shared by every kernel of the step; the per-kernel
 // source/receiver lists are filled by kernel_params.
 template <typename T>
-awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
+awc::StepParams<T> step_params(const awc_plan* P, int64_t it, const StepState& stt) {
   const awc_problem* p = &P->p;
   awc::StepParams<T> S{};
-  T* b[3] = {(T*)P->buf[0], (T*)P->buf[1], (T*)P->buf[2]};
-  // step it (0-based) reads pold = buf[it%3], pcur = buf[(it+1)%3] and writes
-  // pnew = buf[(it+2)%3]: the (pold, pcur, pnew) <- (pcur, pnew, pold)
+  // step it (0-based) reads pold = p_{it-1}, pcur = p_it and writes pnew into
+  // the buffer of p_{it-2}: the (pold, pcur, pnew) <- (pcur, pnew, pold)
   // rotation of forward! (acoustic_3D_xPU.jl:166)
-  S.pold = b[it % 3];
-  S.pcur = b[(it + 1) % 3];
-  S.pnew = b[(it + 2) % 3];
+  S.pold = (const T*)P->buf[stt.ord[1]];
+  S.pcur = (const T*)P->buf[stt.ord[0]];
+  S.pnew = (T*)P->buf[stt.ord[2]];
   S.fact = (const T*)P->fact;
   S.nx = (int32_t)p->nx;
   S.ny = (int32_t)p->ny;
@@ -471,9 +542,9 @@ awc::StepParams<T> step_params(const awc_plan* P, int64_t it) {
     const T* blk = cf + a * (8 * h + 4);
     for (int s = 0; s < 2; ++s) {
       awc::BandSide<T>& B = S.band[a][s];
-      B.psi_old = (const T*)P->psi[a][s][it & 1];
-      B.psi_new = (T*)P->psi[a][s][(it + 1) & 1];
-      B.xi = (T*)P->xi[a][s];
+      B.psi_old = (const T*)P->psi[a][s][stt.psi_par];
+      B.psi_new = (T*)P->psi[a][s][stt.psi_par ^ 1];
+      B.xi = (T*)(stt.xi_par ? P->xi_alt[a][s] : P->xi[a][s]);
       B.a = blk + s * h;
       B.bK = blk + 2 * h + s * h;
       B.ah = blk + 4 * h + s * (h + 1);
@@ -596,7 +667,8 @@ dim3 step_grid(const awc_plan* P) {
 }
 
 uint64_t launch_shape(const awc_plan* P) {
-  return (uint64_t)P->by | ((uint64_t)P->zchunk << 8) | ((uint64_t)(P->szc & 0xff) << 40);
+  return (uint64_t)P->by | ((uint64_t)P->zchunk << 8) | ((uint64_t)(P->szc & 0xff) << 40) |
+         ((uint64_t)(P->depth & 3) << 48) | ((uint64_t)(P->tb_nch & 0x3fff) << 50);
 }
 
 // Buckets the source/receiver nodes by the kernel and block that own them for
@@ -710,12 +782,180 @@ int ensure_maps(awc_plan* P) {
                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   };
-  for (int b = 0; b < 3; ++b)
+  for (int b = 0; b < P->nbuf; ++b)
     if (!make(&P->map_c[b], P->buf[b], box_c) || !make(&P->map_o[b], P->buf[b], box_i))
       return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
   if (!make(&P->map_f, P->fact, box_i))
     return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
   P->maps_by = P->by;
+  return AWC_OK;
+}
+
+// ---- two-step passes (awc_tb.cuh) ------------------------------------------
+
+// Level-2 tile of the two-step kernel: 30 x (TB_ROWS - 2) nodes.
+constexpr int TB_TX = 30, TB_TY = awc::TB_ROWS - 2;
+
+// The number of z chunks the two-step kernel really has when asked for c:
+// chunks of ceil(iz / c) planes cover the iz interior planes in
+// ceil(iz / ceil(iz / c)) chunks.
+int32_t tb_chunks(const awc_plan* P, int64_t c) {
+  const int64_t iz = P->p.nz - 2;
+  c = std::max<int64_t>(1, std::min<int64_t>(c, iz));
+  const int64_t zc = (iz + c - 1) / c;
+  return (int32_t)((iz + zc - 1) / zc);
+}
+
+// Whether the problem can run two-step passes: 3D with every source and
+// receiver on an interior node (the rim of every field then stays zero).
+bool tb_eligible(const awc_plan* P) {
+  if (P->p.ndim != 3) return false;
+  for (const awc::IoRim& e : P->io_nodes) {
+    const int64_t i = e.node % P->px, j = (e.node / P->px) % P->p.ny,
+                  k = e.node / (P->px * P->p.ny);
+    if (i < 1 || i > P->p.nx - 2 || j < 1 || j > P->p.ny - 2 || k < 1 || k > P->p.nz - 2)
+      return false;
+  }
+  return true;
+}
+
+// Whether interior coordinate c of an axis of n nodes lies in an active band.
+bool in_active_band(const awc_plan* P, int a, int64_t c) {
+  const int64_t n = a == 0 ? P->p.nx : a == 1 ? P->p.ny : P->p.nz, h = P->p.halo;
+  if (c < 1 || c > n - 2) return false;
+  if (c <= h) return P->active[a][0] != 0;
+  if (c >= n - h - 1) return P->active[a][1] != 0;
+  return false;
+}
+
+// Tile lists and per-block source/receiver lists of the two-step kernel for
+// the current chunking. Tile (tx, ty) has level-2 origin (1 + 30 tx,
+// 1 + TY ty); it goes to the XY list when its level-1 region (the tile and a
+// ring of one node) meets an active x or y band, else to the Z list.
+int ensure_tb(awc_plan* P) {
+  const uint64_t shape = (uint64_t)P->tb_nch;
+  if (P->tb_io_shape == shape) return AWC_OK;
+  awc_ctx* C = P->ctx;
+  const awc_problem* p = &P->p;
+  const int64_t ntx = (p->nx - 2 + TB_TX - 1) / TB_TX, nty = (p->ny - 2 + TB_TY - 1) / TB_TY;
+  std::vector<int2> tiles[2];
+  std::vector<std::pair<int, int32_t>> where((size_t)(ntx * nty));  // (list, index)
+  for (int64_t ty = 0; ty < nty; ++ty)
+    for (int64_t tx = 0; tx < ntx; ++tx) {
+      const int64_t X0 = 1 + TB_TX * tx, Y0 = 1 + TB_TY * ty;
+      bool xy = false;
+      for (int64_t x = X0 - 1; x <= X0 + TB_TX && !xy; ++x) xy = in_active_band(P, 0, x);
+      for (int64_t y = Y0 - 1; y <= Y0 + TB_TY && !xy; ++y) xy = in_active_band(P, 1, y);
+      where[ty * ntx + tx] = {xy ? 1 : 0, (int32_t)tiles[xy ? 1 : 0].size()};
+      tiles[xy ? 1 : 0].push_back(make_int2((int)X0, (int)Y0));
+    }
+  const int64_t iz = p->nz - 2;
+  P->tb_zc = (int32_t)((iz + P->tb_nch - 1) / P->tb_nch);
+  const int32_t nch = P->tb_nch;  // normalised by tb_chunks: exactly covers iz
+  if ((int64_t)nch * P->tb_zc < iz || (int64_t)(nch - 1) * P->tb_zc >= iz)
+    return set_err(&C->err, AWC_ERR_INVALID, "internal: z chunking does not cover the grid");
+  // entries ((block, plane << 32 | thread), {thread, plane, sgrp, rgrp or -1})
+  std::vector<std::pair<std::pair<int64_t, int64_t>, int4>> ent[2];
+  for (const awc::IoRim& e : P->io_nodes) {
+    const int64_t i = e.node % P->px, j = (e.node / P->px) % p->ny, k = e.node / (P->px * p->ny);
+    const int64_t tx0 = (i - 1) / TB_TX, ty0 = (j - 1) / TB_TY;
+    for (int64_t ty = std::max<int64_t>(ty0 - 1, 0); ty <= std::min(ty0 + 1, nty - 1); ++ty)
+      for (int64_t tx = std::max<int64_t>(tx0 - 1, 0); tx <= std::min(tx0 + 1, ntx - 1); ++tx) {
+        const int64_t X0 = 1 + TB_TX * tx, Y0 = 1 + TB_TY * ty;
+        if (i < X0 - 1 || i > X0 + TB_TX || j < Y0 - 1 || j > Y0 + TB_TY) continue;
+        const bool own_col = i >= X0 && i < X0 + TB_TX && j >= Y0 && j < Y0 + TB_TY;
+        const int thread = (int)((i - (X0 - 1)) + 32 * (j - (Y0 - 1)));
+        const auto& wh = where[ty * ntx + tx];
+        for (int32_t c = 0; c < nch; ++c) {
+          const int64_t k0 = 1 + (int64_t)c * P->tb_zc, k1 = std::min<int64_t>(k0 + P->tb_zc, p->nz - 1);
+          if (k < k0 - 1 || k > k1) continue;
+          const bool own = own_col && k >= k0 && k < k1;
+          const int64_t blk = (int64_t)wh.second * nch + c;
+          ent[wh.first].push_back(
+              {{blk, (k << 32) | thread}, make_int4(thread, (int)k, e.sgrp, own ? e.rgrp : -1)});
+        }
+      }
+  }
+  cudaStream_t st = C->stream;
+  for (int v = 0; v < 2; ++v) {
+    const int64_t nt_ = (int64_t)tiles[v].size();
+    P->tb_ntiles[v] = (int32_t)nt_;
+    if (P->tb_tiles_cap[v] < std::max<int64_t>(nt_, 1)) {
+      P->release(P->tb_tiles[v]);
+      P->tb_tiles[v] = nullptr;
+      P->tb_tiles_cap[v] = 0;
+      if (int rc = P->alloc((void**)&P->tb_tiles[v], std::max<int64_t>(nt_, 1) * sizeof(int2)))
+        return rc;
+      P->tb_tiles_cap[v] = std::max<int64_t>(nt_, 1);
+    }
+    if (nt_ > 0)
+      CUDA_TRY(&C->err, cudaMemcpyAsync(P->tb_tiles[v], tiles[v].data(), nt_ * sizeof(int2),
+                                        cudaMemcpyHostToDevice, st));
+    const int64_t nblk = nt_ * nch;
+    auto& E = ent[v];
+    std::sort(E.begin(), E.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<int32_t> off((size_t)nblk + 1, 0);
+    std::vector<int4> flat(E.size());
+    for (size_t n = 0; n < E.size(); ++n) {
+      off[E[n].first.first + 1]++;
+      flat[n] = E[n].second;
+    }
+    for (int64_t b = 0; b < nblk; ++b) off[b + 1] += off[b];
+    auto& S = P->tb_io[v];
+    if (S.cap < nblk + 1) {
+      P->release(S.blk_off);
+      S.blk_off = nullptr;
+      S.cap = 0;
+      if (int rc = P->alloc((void**)&S.blk_off, (nblk + 1) * 4)) return rc;
+      S.cap = nblk + 1;
+    }
+    // every node appears in at most 4 tiles x 2 chunks
+    const int64_t ecap = std::max<int64_t>((int64_t)flat.size(), 1);
+    if (S.ecap < ecap) {
+      P->release(S.ent);
+      S.ent = nullptr;
+      S.ecap = 0;
+      if (int rc = P->alloc((void**)&S.ent, ecap * sizeof(int4))) return rc;
+      S.ecap = ecap;
+    }
+    CUDA_TRY(&C->err, cudaMemcpyAsync(S.blk_off, off.data(), off.size() * 4,
+                                      cudaMemcpyHostToDevice, st));
+    if (!flat.empty())
+      CUDA_TRY(&C->err, cudaMemcpyAsync(S.ent, flat.data(), flat.size() * sizeof(int4),
+                                        cudaMemcpyHostToDevice, st));
+  }
+  CUDA_TRY(&C->err, cudaStreamSynchronize(st));
+  P->tb_io_shape = shape;
+  return AWC_OK;
+}
+
+// Tensor maps of the two-step kernel for every field buffer: the p_s box
+// (40 x (TB_ROWS + 2)) and the p_{s-1} box (40 x TB_ROWS), and fact's.
+int ensure_tb_maps(awc_plan* P) {
+  if (P->tb_maps) return AWC_OK;
+  awc_ctx* C = P->ctx;
+  const awc_problem* p = &P->p;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = awc::tensor_map_encoder();
+  if (!enc) return set_err(&C->err, AWC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  const CUtensorMapDataType dt =
+      p->precision == AWC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dims[3] = {(cuuint64_t)p->nx, (cuuint64_t)p->ny, (cuuint64_t)p->nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)(P->px * P->esz), (cuuint64_t)(P->px * p->ny * P->esz)};
+  constexpr int BX = awc::TbTile<float, awc::TB_ROWS>::BX;
+  const cuuint32_t box_pt[3] = {BX, awc::TB_ROWS + 2, 1};
+  const cuuint32_t box_in[3] = {BX, awc::TB_ROWS, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  auto make = [&](CUtensorMap* m, void* base, const cuuint32_t* box) -> bool {
+    return enc(m, dt, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  for (int b = 0; b < P->nbuf; ++b)
+    if (!make(&P->tb_map_pt[b], P->buf[b], box_pt) || !make(&P->tb_map_in[b], P->buf[b], box_in))
+      return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
+  if (!make(&P->tb_map_f, P->fact, box_in))
+    return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
+  P->tb_maps = true;
   return AWC_OK;
 }
 
@@ -738,23 +978,25 @@ int init_kernel_attrs(std::string* err) {
   AWC_ATTR(double, 4);
   AWC_ATTR(double, 8);
 #undef AWC_ATTR
+  CUDA_TRY(err, awc::tb_init_attrs());
   return AWC_OK;
 }
 
 template <typename T, int TY>
-void launch_core(awc_plan* P, int64_t it, const awc::StepParams<T>& S, dim3 grid, cudaStream_t st) {
+void launch_core(awc_plan* P, const StepState& stt, const awc::StepParams<T>& S, dim3 grid,
+                 cudaStream_t st) {
   awc::step3d_core<T, TY, stages<T>()><<<grid, dim3(32, TY), core_smem<T, TY>(), st>>>(
-      P->map_c[(it + 1) % 3], P->map_o[it % 3], P->map_f, S);
+      P->map_c[stt.ord[0]], P->map_o[stt.ord[1]], P->map_f, S);
 }
 
 // One time step. 3D: the shell kernel on the context's second stream and the
 // core kernel on its main stream, forked from and joined back into the main
 // stream (parallel branches once captured in a graph). 2D: one kernel.
 template <typename T>
-int launch_step(awc_plan* P, int64_t it, cudaStream_t st) {
+int launch_step(awc_plan* P, int64_t it, const StepState& stt, cudaStream_t st) {
   awc_ctx* C = P->ctx;
   const awc_problem* p = &P->p;
-  awc::StepParams<T> S = step_params<T>(P, it);
+  awc::StepParams<T> S = step_params<T>(P, it, stt);
   if (p->ndim == 2) {
     kernel_params(P, 0, S);
     awc::step2d<T><<<step_grid(P), dim3(32, 8), 0, st>>>(S);
@@ -779,9 +1021,9 @@ int launch_step(awc_plan* P, int64_t it, cudaStream_t st) {
       kernel_params(P, 0, S);
       const dim3 grid = step_grid(P);
       switch (P->by) {
-        case 4: launch_core<T, 2>(P, it, S, grid, st); break;
-        case 8: launch_core<T, 4>(P, it, S, grid, st); break;
-        case 16: launch_core<T, 8>(P, it, S, grid, st); break;
+        case 4: launch_core<T, 2>(P, stt, S, grid, st); break;
+        case 8: launch_core<T, 4>(P, stt, S, grid, st); break;
+        case 16: launch_core<T, 8>(P, stt, S, grid, st); break;
         default: return set_err(&C->err, AWC_ERR_INVALID, "unsupported tile height %d", P->by);
       }
     }
@@ -796,15 +1038,131 @@ int launch_step(awc_plan* P, int64_t it, cudaStream_t st) {
   return AWC_OK;
 }
 
-int launch_range(awc_plan* P, int64_t start, int64_t n, cudaStream_t st) {
-  for (int64_t it = start; it < start + n; ++it) {
-    int rc = P->p.precision == AWC_F64 ? launch_step<double>(P, it, st) : launch_step<float>(P, it, st);
-    if (rc) return rc;
-    if (P->keep && it >= P->keep_first && it < P->keep_first + P->keep_count)
-      CUDA_TRY(&P->ctx->err, cudaMemcpyAsync(P->keep[it - P->keep_first], P->buf[(it + 2) % 3],
-                                             P->NP * P->esz, cudaMemcpyDeviceToDevice, st));
+// Parameters of the two-step pass that starts after step `it` - 1 (it is the
+// 0-based index of its first step) in state `stt`.
+template <typename T>
+awc::TbParams<T> tb_params(const awc_plan* P, int64_t it, const StepState& stt) {
+  const awc_problem* p = &P->p;
+  awc::TbParams<T> Q{};
+  Q.pold = (const T*)P->buf[stt.ord[1]];
+  Q.pcur = (const T*)P->buf[stt.ord[0]];
+  Q.p1 = (T*)P->buf[stt.ord[2]];
+  Q.p2 = (T*)P->buf[stt.ord[3]];
+  Q.fact = (const T*)P->fact;
+  Q.nx = (int32_t)p->nx;
+  Q.ny = (int32_t)p->ny;
+  Q.nz = (int32_t)p->nz;
+  Q.halo = p->halo;
+  Q.px = P->px;
+  Q.plane = P->px * p->ny;
+  const double d[3] = {p->dx, p->dy, p->dz};
+  for (int a = 0; a < 3; ++a) {
+    Q.inv_d[a] = (T)(1.0 / d[a]);
+    Q.inv_d2[a] = (T)(1.0 / (d[a] * d[a]));
+  }
+  const int64_t h = p->halo;
+  const T* cf = (const T*)P->coef;
+  for (int a = 0; a < 3; ++a) {
+    const T* blk = cf + a * (8 * h + 4);
+    awc::TbAxis<T>& X = Q.ax[a];
+    X.psi_in = (const T*)P->psi[a][0][stt.psi_par];
+    X.psi_out = (T*)P->psi[a][0][stt.psi_par ^ 1];
+    X.xi_in = (const T*)(stt.xi_par ? P->xi_alt[a][0] : P->xi[a][0]);
+    X.xi_out = (T*)(stt.xi_par ? P->xi[a][0] : P->xi_alt[a][0]);
+    X.a = blk;
+    X.bK = blk + 2 * h;
+    X.ah = blk + 4 * h;
+    X.bKh = blk + 4 * h + 2 * (h + 1);
+    X.psi_side = P->psi_side[a];
+    X.xi_side = P->xi_side[a];
+    for (int sd = 0; sd < 2; ++sd) Q.active[a][sd] = P->active[a][sd];
+    const int64_t n = a == 0 ? p->nx : a == 1 ? p->ny : p->nz;
+    Q.first_r[a] = (int32_t)std::max<int64_t>(n - h - 1, h + 1);
+  }
+  Q.damp_all = P->has_core ? 0 : 1;
+  Q.it = (int32_t)it;
+  Q.err = P->err_flag;
+  Q.io.src_off = P->src_off;
+  Q.io.src_ids = P->src_ids;
+  Q.io.rec_off = P->rec_off;
+  Q.io.rec_ids = P->rec_ids;
+  Q.io.stf = (const T*)P->stf;
+  Q.io.nsrc = (int32_t)p->nsrc;
+  Q.io.nrec = (int32_t)p->nrec;
+  Q.io.traces = (T*)P->traces;
+  Q.nch = P->tb_nch;
+  Q.zc = P->tb_zc;
+  Q.wait_rounds = P->wait_rounds;
+  Q.wait_ns = P->wait_ns;
+  Q.withhold = P->withhold;
+  return Q;
+}
+
+// One two-step pass (steps it and it + 1): the XY tiles on the second stream
+// and the Z tiles on the main one, as parallel branches like a 3D step.
+template <typename T>
+int launch_pass2(awc_plan* P, int64_t it, const StepState& stt, cudaStream_t st) {
+  awc_ctx* C = P->ctx;
+  awc::TbParams<T> Q = tb_params<T>(P, it, stt);
+  const bool i64 = P->NP > (int64_t)INT32_MAX;
+  const bool both = P->tb_ntiles[0] > 0 && P->tb_ntiles[1] > 0;
+  if (both) {
+    CUDA_TRY(&C->err, cudaEventRecord(C->ev_fork, st));
+    CUDA_TRY(&C->err, cudaStreamWaitEvent(C->stream2, C->ev_fork, 0));
+  }
+  for (int v = 1; v >= 0; --v) {
+    if (P->tb_ntiles[v] == 0) continue;
+    Q.tiles = P->tb_tiles[v];
+    Q.io.blk_off = P->tb_io[v].blk_off;
+    Q.io.ent = P->tb_io[v].ent;
+    const unsigned nb = (unsigned)((int64_t)P->tb_ntiles[v] * P->tb_nch);
+    const cudaError_t e =
+        awc::tb_launch<T>(Q, v == 1, i64, P->tb_map_pt[stt.ord[0]], P->tb_map_in[stt.ord[1]],
+                          P->tb_map_f, nb, (v == 1 && both) ? C->stream2 : st);
+    if (e != cudaSuccess)
+      return set_err(&C->err, AWC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
+  }
+  if (both) {
+    CUDA_TRY(&C->err, cudaEventRecord(C->ev_join, C->stream2));
+    CUDA_TRY(&C->err, cudaStreamWaitEvent(st, C->ev_join, 0));
   }
   return AWC_OK;
+}
+
+// Whether the launch sequence of this plan advances two steps per pass.
+bool two_step(const awc_plan* P) { return P->depth == 2 && !P->keep; }
+
+// Launches steps [start, start + n) from state `stt` (updated to the state
+// after them): two-step passes while two steps remain at depth 2, else
+// one-step launches.
+int launch_range(awc_plan* P, int64_t start, int64_t n, StepState& stt, cudaStream_t st) {
+  const bool f64 = P->p.precision == AWC_F64;
+  for (int64_t it = start; it < start + n;) {
+    int rc;
+    if (two_step(P) && it + 1 < start + n) {
+      rc = f64 ? launch_pass2<double>(P, it, stt, st) : launch_pass2<float>(P, it, stt, st);
+      if (rc) return rc;
+      stt.pass2();
+      it += 2;
+      continue;
+    }
+    rc = f64 ? launch_step<double>(P, it, stt, st) : launch_step<float>(P, it, stt, st);
+    if (rc) return rc;
+    if (P->keep && it >= P->keep_first && it < P->keep_first + P->keep_count)
+      CUDA_TRY(&P->ctx->err, cudaMemcpyAsync(P->keep[it - P->keep_first], P->buf[stt.ord[2]],
+                                             P->NP * P->esz, cudaMemcpyDeviceToDevice, st));
+    stt.step1();
+    ++it;
+  }
+  return AWC_OK;
+}
+
+// Kernel launches of n steps from the current state.
+int64_t launch_count(const awc_plan* P, int64_t n) {
+  const int64_t one = (P->p.ndim == 3 && P->has_core && P->nbox > 0) ? 2 : 1;
+  if (!two_step(P)) return one * n;
+  const int64_t per_pass = (P->tb_ntiles[0] > 0 ? 1 : 0) + (P->tb_ntiles[1] > 0 ? 1 : 0);
+  return per_pass * (n / 2) + one * (n % 2);
 }
 
 // Everything a launch sequence depends on besides the step index.
@@ -812,6 +1170,7 @@ int prepare_launch(awc_plan* P) {
   int rc;
   if ((rc = ensure_io(P))) return rc;
   if (P->p.ndim == 3 && P->has_core && (rc = ensure_maps(P))) return rc;
+  if (two_step(P) && ((rc = ensure_tb(P)) || (rc = ensure_tb_maps(P)))) return rc;
   return AWC_OK;
 }
 
@@ -827,7 +1186,12 @@ awc_plan::GraphKey config_key(const awc_plan* P) {
   for (int w = 0; w < 2; ++w) {
     k.do_rim[w] = P->io_k[w].do_rim;
     k.blk_off[w] = P->io_k[w].blk_off;
+    k.blk_off[2 + w] = P->tb_io[w].blk_off;
+    k.tiles[w] = P->tb_tiles[w];
   }
+  k.wait[0] = P->wait_rounds;
+  k.wait[1] = P->wait_ns;
+  k.wait[2] = P->withhold;
   return k;
 }
 
@@ -838,14 +1202,16 @@ int get_graph(awc_plan* P, int64_t start, int64_t n, cudaGraphExec_t* out) {
     P->drop_graphs();
     P->graph_key = key;
   }
-  auto f = P->graphs.find({start, n});
+  const std::array<int64_t, 3> gk{start, n, P->state.code()};
+  auto f = P->graphs.find(gk);
   if (f != P->graphs.end()) {
     *out = f->second;
     return AWC_OK;
   }
   cudaGraph_t g = nullptr;
   CUDA_TRY(&C->err, cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = launch_range(P, start, n, C->stream);
+  StepState stt = P->state;
+  int rc = launch_range(P, start, n, stt, C->stream);
   cudaError_t e = cudaStreamEndCapture(C->stream, &g);
   if (rc) {
     if (g) cudaGraphDestroy(g);
@@ -858,7 +1224,7 @@ int get_graph(awc_plan* P, int64_t start, int64_t n, cudaGraphExec_t* out) {
   cudaGraphDestroy(g);
   if (e != cudaSuccess)
     return set_err(&C->err, AWC_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-  P->graphs[{start, n}] = ex;
+  P->graphs[gk] = ex;
   *out = ex;
   return AWC_OK;
 }
@@ -1004,7 +1370,10 @@ PlanView plan_view(awc_plan* P) {
   return V;
 }
 
-void plan_set_step(awc_plan* P, int64_t step) { P->step = step; }
+void plan_set_step(awc_plan* P, int64_t step) {
+  P->step = step;
+  P->state = StepState::after_steps(step);
+}
 
 void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count) {
   P->keep = dst;
@@ -1155,19 +1524,23 @@ int awc_plan_reset(awc_plan* P) {
   const awc_problem* p = &P->p;
   cudaStream_t st = C->stream;
   CUDA_TRY(&C->err, cudaSetDevice(C->device));
-  for (int b = 0; b < 3; ++b)
+  for (int b = 0; b < P->nbuf; ++b)
     CUDA_TRY(&C->err, cudaMemsetAsync(P->buf[b], 0, P->NP * P->esz, st));
   for (int a = 0; a < p->ndim; ++a)
     for (int s = 0; s < 2; ++s) {
       const int64_t cs = cross_section(p, a);
       for (int par = 0; par < 2; ++par)
         CUDA_TRY(&C->err, cudaMemsetAsync(P->psi[a][s][par], 0, (p->halo + 1) * cs * P->esz, st));
-      if (p->halo > 0)
+      if (p->halo > 0) {
         CUDA_TRY(&C->err, cudaMemsetAsync(P->xi[a][s], 0, p->halo * cs * P->esz, st));
+        if (P->xi_alt[a][s])
+          CUDA_TRY(&C->err, cudaMemsetAsync(P->xi_alt[a][s], 0, p->halo * cs * P->esz, st));
+      }
     }
   if (p->nt * p->nrec > 0)
     CUDA_TRY(&C->err, cudaMemsetAsync(P->traces, 0, p->nt * p->nrec * P->esz, st));
   P->step = 0;
+  P->state = StepState();
   return AWC_OK;
 }
 
@@ -1187,13 +1560,26 @@ int awc_plan_run(awc_plan* P, int64_t nsteps, int32_t use_graph, float* ms) {
   CUDA_TRY(&C->err, cudaEventRecord(C->ev0, C->stream));
   if (use_graph) {
     CUDA_TRY(&C->err, cudaGraphLaunch(ex, C->stream));
-  } else if ((rc = launch_range(P, P->step, n, C->stream))) {
-    return rc;
+  }
+  StepState end = P->state;
+  if (!use_graph) {
+    if ((rc = launch_range(P, P->step, n, end, C->stream))) return rc;
+  } else {
+    for (int64_t it = P->step; it < P->step + n;) {  // the state the graph leaves
+      if (two_step(P) && it + 1 < P->step + n) {
+        end.pass2();
+        it += 2;
+      } else {
+        end.step1();
+        ++it;
+      }
+    }
   }
   CUDA_TRY(&C->err, cudaEventRecord(C->ev1, C->stream));
   CUDA_TRY(&C->err, cudaEventSynchronize(C->ev1));
   if (ms) CUDA_TRY(&C->err, cudaEventElapsedTime(ms, C->ev0, C->ev1));
   P->step += n;
+  P->state = end;
   return check_device_flag(P);
 }
 
@@ -1220,8 +1606,8 @@ int awc_plan_field(awc_plan* P, double* out) {
   if (!P || !out) return set_err(nullptr, AWC_ERR_INVALID, "plan/out is NULL");
   awc_ctx* C = P->ctx;
   CUDA_TRY(&C->err, cudaSetDevice(C->device));
-  // after s steps the latest new field is buf[(s+1)%3] (the reference's pcur)
-  const void* cur = P->buf[(P->step + 1) % 3];
+  // the latest new field (the reference's pcur)
+  const void* cur = P->buf[P->state.ord[0]];
   const int blocks = grid_for(C, P->N, 256);
   if (P->p.precision == AWC_F64)
     awc::unpitch<double><<<blocks, 256, 0, C->stream>>>((const double*)cur, P->staging, P->N, P->p.nx, P->px);
@@ -1262,6 +1648,45 @@ int awc_plan_get_launch(const awc_plan* P, int32_t* tile_y, int32_t* zchunk, int
   return AWC_OK;
 }
 
+int awc_plan_set_blocking(awc_plan* P, int32_t depth, int32_t zchunks) {
+  if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
+  if (depth != 1 && depth != 2)
+    return set_err(&P->ctx->err, AWC_ERR_INVALID, "depth must be 1 or 2");
+  if (zchunks < 1) return set_err(&P->ctx->err, AWC_ERR_INVALID, "zchunks must be >= 1");
+  if (depth == 2 && !tb_eligible(P))
+    return set_err(&P->ctx->err, AWC_ERR_INVALID,
+                   "two-step passes need a 3D problem whose sources and receivers are all "
+                   "interior nodes");
+  P->depth = depth;
+  if (P->p.ndim == 3) P->tb_nch = tb_chunks(P, zchunks);
+  return AWC_OK;
+}
+
+int awc_plan_get_blocking(const awc_plan* P, int32_t* depth, int32_t* zchunks) {
+  if (!P || !depth || !zchunks) return set_err(nullptr, AWC_ERR_INVALID, "NULL argument");
+  *depth = P->depth;
+  *zchunks = P->tb_nch;
+  return AWC_OK;
+}
+
+int awc_plan_set_wait(awc_plan* P, int32_t rounds, int32_t round_ns, int32_t withhold) {
+  if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
+  if (rounds < 1 || round_ns < 1 || round_ns > 10000000 || withhold < -1)
+    return set_err(&P->ctx->err, AWC_ERR_INVALID,
+                   "rounds >= 1, round_ns in [1, 1e7] and withhold >= -1 are required");
+  P->wait_rounds = rounds;
+  P->wait_ns = round_ns;
+  P->withhold = withhold;
+  return AWC_OK;
+}
+
+int64_t awc_plan_launch_count(const awc_plan* P, int64_t nsteps) {
+  if (!P || nsteps < 0) return -1;
+  // the tile lists (how many launches a pass has) follow the blocking
+  if (two_step(P) && ensure_tb(const_cast<awc_plan*>(P)) != AWC_OK) return -1;
+  return launch_count(P, std::min<int64_t>(nsteps, P->p.nt - P->step));
+}
+
 namespace {
 // Device time per step [ms] of the current launch shape: the faster of two
 // runs of n steps (the state is reset before and is garbage after).
@@ -1269,7 +1694,7 @@ int time_shape(awc_plan* P, int64_t n, float* per) {
   int rc;
   *per = 1e30f;
   for (int rep = 0; rep < 2; ++rep) {
-    if ((rc = awc_plan_reset(P)) || (rc = awc_plan_run(P, 1, 0, nullptr))) return rc;  // warm-up
+    if ((rc = awc_plan_reset(P)) || (rc = awc_plan_run(P, 2, 0, nullptr))) return rc;  // warm-up
     float ms = 0.f;
     if ((rc = awc_plan_run(P, n, 0, &ms))) return rc;
     *per = std::min(*per, ms / (float)n);
@@ -1286,8 +1711,14 @@ int awc_plan_autotune(awc_plan* P, int64_t steps, float* best_ms_per_step) {
     if (best_ms_per_step) *best_ms_per_step = 0.f;
     return AWC_OK;
   }
-  const int64_t n = std::min<int64_t>(steps, P->p.nt - 1);
+  // an even number of timed steps (two-step passes), after 2 warm-up steps
+  const int64_t n = std::max<int64_t>(2, std::min<int64_t>(steps, P->p.nt - 2) / 2 * 2);
+  if (P->p.nt < n + 2) {
+    if (best_ms_per_step) *best_ms_per_step = 0.f;
+    return AWC_OK;
+  }
   int rc;
+  P->depth = 1;
   // phase 1: core tile height and z chunk
   std::vector<std::pair<int32_t, int32_t>> cands;
   for (int by : {4, 8, 16})
@@ -1324,6 +1755,30 @@ int awc_plan_autotune(awc_plan* P, int64_t steps, float* best_ms_per_step) {
     }
     P->szc = wz;
     box_blocks(P);
+  }
+  // phase 3: two-step passes, z chunks per column tile
+  if (tb_eligible(P)) {
+    const int64_t ntiles = ((P->p.nx - 2 + TB_TX - 1) / TB_TX) * ((P->p.ny - 2 + TB_TY - 1) / TB_TY);
+    const int64_t resident = (int64_t)C->num_sms * awc::tb_occupancy(P->p.precision == AWC_F64, false);
+    std::vector<int32_t> chs;
+    for (double waves : {0.5, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0}) {
+      const int32_t c = tb_chunks(P, std::llround(waves * (double)resident / (double)ntiles));
+      if (std::find(chs.begin(), chs.end(), c) == chs.end()) chs.push_back(c);
+    }
+    int32_t wdepth = 1, wch = P->tb_nch;
+    for (int32_t c : chs) {
+      P->depth = 2;
+      P->tb_nch = c;
+      float per = 0.f;
+      if ((rc = time_shape(P, n, &per))) return rc;
+      if (per < best) {
+        best = per;
+        wdepth = 2;
+        wch = c;
+      }
+    }
+    P->depth = wdepth;
+    P->tb_nch = wch;
   }
   if (best_ms_per_step) *best_ms_per_step = best;
   return awc_plan_reset(P);

@@ -48,6 +48,8 @@ def parse_args():
                     help="device-resident leg only (no e2e, FP64 or CPU legs); for profiling")
     ap.add_argument("--launch", default=None,
                     help="tile_y,zchunk,band_zchunk of the 3D step instead of autotuning")
+    ap.add_argument("--blocking", default=None, metavar="DEPTH,ZCHUNKS",
+                    help="fixed time blocking of the 3D leg (default: the autotuner's choice)")
     ap.add_argument("--batch-only", default=None, metavar="TILE_Y,BLOCKS_PER_SM",
                     help="profiling: only the batched 2D workload at --nt steps and this launch "
                          "shape (one eager run, no timing line)")
@@ -404,7 +406,10 @@ def main():
         plan.set_launch(*[int(x) for x in args.launch.split(",")])
     else:
         plan.autotune(40)  # launch shape picked on this data, before any timing
+    if args.blocking:
+        plan.set_blocking(*[int(x) for x in args.blocking.split(",")])
     launch = plan.get_launch()
+    depth, tb_zchunks = plan.get_blocking()
 
     def shot():
         plan.reset()
@@ -416,7 +421,8 @@ def main():
         ms = timed(shot, args.steps)
     clocks = clk.summary()
     traces_dev = plan.traces()
-    launches = args.steps * nt * plan.launches_per_step
+    plan.reset()
+    launches = args.steps * plan.launch_count(nt)
     plan.close()
 
     ab = a_eff(pkg, p)
@@ -440,7 +446,8 @@ def main():
                          " MB each, no flush needed)",
                    "parallelism": f"shots{world}",
                    "launch": {"core_tile": [64, launch[0]], "core_zchunk": launch[1],
-                              "band_zchunk": launch[2]}},
+                              "band_zchunk": launch[2], "depth": depth,
+                              "depth2_zchunks": tb_zchunks}},
         "gcells_per_s": world * interior_cells(p) / t_ts / 1e9,
         "us_per_timestep": t_ts * 1e6,
         "a_eff_bytes_per_timestep": ab,

@@ -158,6 +158,32 @@ int awc_plan_get_launch(const awc_plan* plan, int32_t* tile_y, int32_t* zchunk,
  * data, keeps the fastest, and resets the state. Writes the best time per
  * step [ms] to best_ms_per_step when not NULL. */
 int awc_plan_autotune(awc_plan* plan, int64_t steps, float* best_ms_per_step);
+/* Time blocking of a 3D plan: `depth` time steps per kernel pass, 1 or 2.
+ * At depth 2 one pass of one kernel advances two steps (two launches per
+ * pass, run as parallel graph branches: the column tiles that meet an x or y
+ * CPML band, and the others). A block stages p_s, p_{s-1} and fact of a
+ * 30 x 14 column tile plus a one-node ring through TMA, computes step s+1 on
+ * the tile and its ring and step s+2 on the tile, streaming one of `zchunks`
+ * chunks of z planes; per node and two steps the fields cost 5 words of HBM
+ * traffic instead of 8, and the CPML state one read and one write instead of
+ * two. Results are bitwise those of depth 1; an odd step count ends with a
+ * one-step launch. Depth 2 needs a 3D problem whose sources and receivers are
+ * all interior nodes (AWC_ERR_INVALID otherwise). The state is kept.
+ * awc_plan_autotune times depth 2 as well and keeps the faster. No
+ * counterpart in the reference, whose forward! advances one step per
+ * launch sequence (src/shared/acoustic_3D_xPU.jl:124-167). */
+int awc_plan_set_blocking(awc_plan* plan, int32_t depth, int32_t zchunks);
+int awc_plan_get_blocking(const awc_plan* plan, int32_t* depth, int32_t* zchunks);
+/* Kernel launches that a run of nsteps steps from the plan's current step
+ * issues (for launch accounting at either depth); -1 on a bad argument. */
+int64_t awc_plan_launch_count(const awc_plan* plan, int64_t nsteps);
+/* Bounded waits of the two-step kernel's TMA pipeline: a wait gives up after
+ * `rounds` try-waits of at most round_ns nanoseconds each (default 4096 x
+ * 1 ms), and the run returns AWC_ERR_TIMEOUT with the context still usable.
+ * withhold >= 0 exists to test that path: the producer of every block skips
+ * the plane load with that index, so that its consumers' wait runs out;
+ * -1 (the default) loads every plane. */
+int awc_plan_set_wait(awc_plan* plan, int32_t rounds, int32_t round_ns, int32_t withhold);
 
 /* ---- Batched 2D shots ----------------------------------------------------
  * Many shots over several 2D velocity models of uneven size advance together:
