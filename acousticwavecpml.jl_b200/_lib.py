@@ -109,8 +109,10 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32)]),
     "awc_plan_autotune": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_float)]),
-    "awc_plan_set_blocking": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32]),
+    "awc_plan_set_blocking": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_int32]),
     "awc_plan_get_blocking": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int32),
+                                             ctypes.POINTER(ctypes.c_int32),
                                              ctypes.POINTER(ctypes.c_int32)]),
     "awc_plan_launch_count": (ctypes.c_int64, [_vp, ctypes.c_int64]),
     "awc_plan_set_wait": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),

@@ -144,17 +144,19 @@ class Plan:
                                              ctypes.byref(bz)), self.ctx.handle)
         return ty.value, zc.value, bz.value
 
-    def set_blocking(self, depth, zchunks=2):
-        """Time steps per kernel pass (1 or 2) and z chunks per column tile of
-        the two-step kernel; results do not depend on either."""
-        check(_lib.lib().awc_plan_set_blocking(self._h, int(depth), int(zchunks)),
+    def set_blocking(self, depth, zchunks=2, rows=16):
+        """Time steps per kernel pass (1 or 2), and the two-step kernel's z
+        chunks per column tile and region rows (8 or 16); results do not
+        depend on any of them."""
+        check(_lib.lib().awc_plan_set_blocking(self._h, int(depth), int(rows), int(zchunks)),
               self.ctx.handle)
 
     def get_blocking(self):
-        d, z = ctypes.c_int32(), ctypes.c_int32()
-        check(_lib.lib().awc_plan_get_blocking(self._h, ctypes.byref(d), ctypes.byref(z)),
-              self.ctx.handle)
-        return d.value, z.value
+        """(depth, zchunks, rows)."""
+        d, r, z = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        check(_lib.lib().awc_plan_get_blocking(self._h, ctypes.byref(d), ctypes.byref(r),
+                                               ctypes.byref(z)), self.ctx.handle)
+        return d.value, z.value, r.value
 
     def launch_count(self, nsteps=None):
         """Kernel launches a run of nsteps (default: the remaining steps) issues."""

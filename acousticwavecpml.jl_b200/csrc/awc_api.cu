@@ -247,8 +247,9 @@ struct awc_plan {
   int64_t tb_tiles_cap[2] = {};
   IoSet tb_io[2];
   uint64_t tb_io_shape = ~0ull;
+  int32_t tb_rows = 16;      // rows of the level-1 region (8 or 16)
   CUtensorMap tb_map_pt[4], tb_map_in[4], tb_map_f;
-  bool tb_maps = false;
+  int32_t tb_maps_rows = 0;  // rows the tensor maps were encoded for
   int32_t wait_rounds = 4096, wait_ns = 1000000, withhold = -1;
   // run state
   int64_t step = 0;
@@ -668,7 +669,8 @@ dim3 step_grid(const awc_plan* P) {
 
 uint64_t launch_shape(const awc_plan* P) {
   return (uint64_t)P->by | ((uint64_t)P->zchunk << 8) | ((uint64_t)(P->szc & 0xff) << 40) |
-         ((uint64_t)(P->depth & 3) << 48) | ((uint64_t)(P->tb_nch & 0x3fff) << 50);
+         ((uint64_t)(P->depth & 3) << 48) | ((uint64_t)(P->tb_nch & 0xfff) << 50) |
+         ((uint64_t)(P->tb_rows == 8 ? 1 : 0) << 62);
 }
 
 // Buckets the source/receiver nodes by the kernel and block that own them for
@@ -793,8 +795,10 @@ int ensure_maps(awc_plan* P) {
 
 // ---- two-step passes (awc_tb.cuh) ------------------------------------------
 
-// Level-2 tile of the two-step kernel: 30 x (TB_ROWS - 2) nodes.
-constexpr int TB_TX = 30, TB_TY = awc::TB_ROWS - 2;
+// Level-2 tile of the two-step kernel: 62 x (rows - 2) nodes; its level-1
+// region adds a ring of one node (64 x rows).
+constexpr int TB_TX = awc::TbTile<float, 16>::TX;
+constexpr int TB_RX = awc::TbTile<float, 16>::RX;
 
 // The number of z chunks the two-step kernel really has when asked for c:
 // chunks of ceil(iz / c) planes cover the iz interior planes in
@@ -833,8 +837,9 @@ bool in_active_band(const awc_plan* P, int a, int64_t c) {
 // 1 + TY ty); it goes to the XY list when its level-1 region (the tile and a
 // ring of one node) meets an active x or y band, else to the Z list.
 int ensure_tb(awc_plan* P) {
-  const uint64_t shape = (uint64_t)P->tb_nch;
+  const uint64_t shape = (uint64_t)P->tb_nch | ((uint64_t)P->tb_rows << 32);
   if (P->tb_io_shape == shape) return AWC_OK;
+  const int64_t TB_TY = P->tb_rows - 2;
   awc_ctx* C = P->ctx;
   const awc_problem* p = &P->p;
   const int64_t ntx = (p->nx - 2 + TB_TX - 1) / TB_TX, nty = (p->ny - 2 + TB_TY - 1) / TB_TY;
@@ -864,7 +869,8 @@ int ensure_tb(awc_plan* P) {
         const int64_t X0 = 1 + TB_TX * tx, Y0 = 1 + TB_TY * ty;
         if (i < X0 - 1 || i > X0 + TB_TX || j < Y0 - 1 || j > Y0 + TB_TY) continue;
         const bool own_col = i >= X0 && i < X0 + TB_TX && j >= Y0 && j < Y0 + TB_TY;
-        const int thread = (int)((i - (X0 - 1)) + 32 * (j - (Y0 - 1)));
+        // the node's index in the level-1 region: 2 x (thread) + (node of its pair)
+        const int thread = (int)((i - (X0 - 1)) + TB_RX * (j - (Y0 - 1)));
         const auto& wh = where[ty * ntx + tx];
         for (int32_t c = 0; c < nch; ++c) {
           const int64_t k0 = 1 + (int64_t)c * P->tb_zc, k1 = std::min<int64_t>(k0 + P->tb_zc, p->nz - 1);
@@ -932,7 +938,7 @@ int ensure_tb(awc_plan* P) {
 // Tensor maps of the two-step kernel for every field buffer: the p_s box
 // (40 x (TB_ROWS + 2)) and the p_{s-1} box (40 x TB_ROWS), and fact's.
 int ensure_tb_maps(awc_plan* P) {
-  if (P->tb_maps) return AWC_OK;
+  if (P->tb_maps_rows == P->tb_rows) return AWC_OK;
   awc_ctx* C = P->ctx;
   const awc_problem* p = &P->p;
   PFN_cuTensorMapEncodeTiled_v12000 enc = awc::tensor_map_encoder();
@@ -941,9 +947,9 @@ int ensure_tb_maps(awc_plan* P) {
       p->precision == AWC_F64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   const cuuint64_t dims[3] = {(cuuint64_t)p->nx, (cuuint64_t)p->ny, (cuuint64_t)p->nz};
   const cuuint64_t strides[2] = {(cuuint64_t)(P->px * P->esz), (cuuint64_t)(P->px * p->ny * P->esz)};
-  constexpr int BX = awc::TbTile<float, awc::TB_ROWS>::BX;
-  const cuuint32_t box_pt[3] = {BX, awc::TB_ROWS + 2, 1};
-  const cuuint32_t box_in[3] = {BX, awc::TB_ROWS, 1};
+  constexpr int BX = awc::TbTile<float, 16>::BX;
+  const cuuint32_t box_pt[3] = {BX, (cuuint32_t)P->tb_rows + 2, 1};
+  const cuuint32_t box_in[3] = {BX, (cuuint32_t)P->tb_rows, 1};
   const cuuint32_t es[3] = {1, 1, 1};
   auto make = [&](CUtensorMap* m, void* base, const cuuint32_t* box) -> bool {
     return enc(m, dt, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -955,7 +961,7 @@ int ensure_tb_maps(awc_plan* P) {
       return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
   if (!make(&P->tb_map_f, P->fact, box_in))
     return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
-  P->tb_maps = true;
+  P->tb_maps_rows = P->tb_rows;
   return AWC_OK;
 }
 
@@ -1117,8 +1123,9 @@ int launch_pass2(awc_plan* P, int64_t it, const StepState& stt, cudaStream_t st)
     Q.io.ent = P->tb_io[v].ent;
     const unsigned nb = (unsigned)((int64_t)P->tb_ntiles[v] * P->tb_nch);
     const cudaError_t e =
-        awc::tb_launch<T>(Q, v == 1, i64, P->tb_map_pt[stt.ord[0]], P->tb_map_in[stt.ord[1]],
-                          P->tb_map_f, nb, (v == 1 && both) ? C->stream2 : st);
+        awc::tb_launch<T>(Q, v == 1, i64, P->tb_rows, P->tb_map_pt[stt.ord[0]],
+                          P->tb_map_in[stt.ord[1]], P->tb_map_f, nb,
+                          (v == 1 && both) ? C->stream2 : st);
     if (e != cudaSuccess)
       return set_err(&C->err, AWC_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e));
   }
@@ -1648,23 +1655,26 @@ int awc_plan_get_launch(const awc_plan* P, int32_t* tile_y, int32_t* zchunk, int
   return AWC_OK;
 }
 
-int awc_plan_set_blocking(awc_plan* P, int32_t depth, int32_t zchunks) {
+int awc_plan_set_blocking(awc_plan* P, int32_t depth, int32_t rows, int32_t zchunks) {
   if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
   if (depth != 1 && depth != 2)
     return set_err(&P->ctx->err, AWC_ERR_INVALID, "depth must be 1 or 2");
+  if (rows != 8 && rows != 16) return set_err(&P->ctx->err, AWC_ERR_INVALID, "rows must be 8 or 16");
   if (zchunks < 1) return set_err(&P->ctx->err, AWC_ERR_INVALID, "zchunks must be >= 1");
   if (depth == 2 && !tb_eligible(P))
     return set_err(&P->ctx->err, AWC_ERR_INVALID,
                    "two-step passes need a 3D problem whose sources and receivers are all "
                    "interior nodes");
   P->depth = depth;
+  P->tb_rows = rows;
   if (P->p.ndim == 3) P->tb_nch = tb_chunks(P, zchunks);
   return AWC_OK;
 }
 
-int awc_plan_get_blocking(const awc_plan* P, int32_t* depth, int32_t* zchunks) {
-  if (!P || !depth || !zchunks) return set_err(nullptr, AWC_ERR_INVALID, "NULL argument");
+int awc_plan_get_blocking(const awc_plan* P, int32_t* depth, int32_t* rows, int32_t* zchunks) {
+  if (!P || !depth || !rows || !zchunks) return set_err(nullptr, AWC_ERR_INVALID, "NULL argument");
   *depth = P->depth;
+  *rows = P->tb_rows;
   *zchunks = P->tb_nch;
   return AWC_OK;
 }
@@ -1758,26 +1768,33 @@ int awc_plan_autotune(awc_plan* P, int64_t steps, float* best_ms_per_step) {
   }
   // phase 3: two-step passes, z chunks per column tile
   if (tb_eligible(P)) {
-    const int64_t ntiles = ((P->p.nx - 2 + TB_TX - 1) / TB_TX) * ((P->p.ny - 2 + TB_TY - 1) / TB_TY);
-    const int64_t resident = (int64_t)C->num_sms * awc::tb_occupancy(P->p.precision == AWC_F64, false);
-    std::vector<int32_t> chs;
-    for (double waves : {0.5, 1.0, 1.5, 2.0, 3.0, 4.0, 6.0}) {
-      const int32_t c = tb_chunks(P, std::llround(waves * (double)resident / (double)ntiles));
-      if (std::find(chs.begin(), chs.end(), c) == chs.end()) chs.push_back(c);
-    }
-    int32_t wdepth = 1, wch = P->tb_nch;
-    for (int32_t c : chs) {
-      P->depth = 2;
-      P->tb_nch = c;
-      float per = 0.f;
-      if ((rc = time_shape(P, n, &per))) return rc;
-      if (per < best) {
-        best = per;
-        wdepth = 2;
-        wch = c;
+    int32_t wdepth = 1, wrows = P->tb_rows, wch = P->tb_nch;
+    for (int32_t rows : {16, 8}) {
+      const int64_t ty = rows - 2;
+      const int64_t ntiles = ((P->p.nx - 2 + TB_TX - 1) / TB_TX) * ((P->p.ny - 2 + ty - 1) / ty);
+      const int64_t resident =
+          (int64_t)C->num_sms * awc::tb_occupancy(P->p.precision == AWC_F64, false, rows);
+      std::vector<int32_t> chs;
+      for (double waves : {1.0, 2.0, 3.0, 4.0, 6.0}) {
+        const int32_t c = tb_chunks(P, std::llround(waves * (double)resident / (double)ntiles));
+        if (std::find(chs.begin(), chs.end(), c) == chs.end()) chs.push_back(c);
+      }
+      for (int32_t c : chs) {
+        P->depth = 2;
+        P->tb_rows = rows;
+        P->tb_nch = c;
+        float per = 0.f;
+        if ((rc = time_shape(P, n, &per))) return rc;
+        if (per < best) {
+          best = per;
+          wdepth = 2;
+          wrows = rows;
+          wch = c;
+        }
       }
     }
     P->depth = wdepth;
+    P->tb_rows = wrows;
     P->tb_nch = wch;
   }
   if (best_ms_per_step) *best_ms_per_step = best;

@@ -48,7 +48,7 @@ def parse_args():
                     help="device-resident leg only (no e2e, FP64 or CPU legs); for profiling")
     ap.add_argument("--launch", default=None,
                     help="tile_y,zchunk,band_zchunk of the 3D step instead of autotuning")
-    ap.add_argument("--blocking", default=None, metavar="DEPTH,ZCHUNKS",
+    ap.add_argument("--blocking", default=None, metavar="DEPTH,ZCHUNKS[,ROWS]",
                     help="fixed time blocking of the 3D leg (default: the autotuner's choice)")
     ap.add_argument("--batch-only", default=None, metavar="TILE_Y,BLOCKS_PER_SM",
                     help="profiling: only the batched 2D workload at --nt steps and this launch "
@@ -409,7 +409,7 @@ def main():
     if args.blocking:
         plan.set_blocking(*[int(x) for x in args.blocking.split(",")])
     launch = plan.get_launch()
-    depth, tb_zchunks = plan.get_blocking()
+    depth, tb_zchunks, tb_rows = plan.get_blocking()
 
     def shot():
         plan.reset()
@@ -447,7 +447,7 @@ def main():
                    "parallelism": f"shots{world}",
                    "launch": {"core_tile": [64, launch[0]], "core_zchunk": launch[1],
                               "band_zchunk": launch[2], "depth": depth,
-                              "depth2_zchunks": tb_zchunks}},
+                              "depth2_zchunks": tb_zchunks, "depth2_rows": tb_rows}},
         "gcells_per_s": world * interior_cells(p) / t_ts / 1e9,
         "us_per_timestep": t_ts * 1e6,
         "a_eff_bytes_per_timestep": ab,

@@ -161,10 +161,11 @@ int awc_plan_autotune(awc_plan* plan, int64_t steps, float* best_ms_per_step);
 /* Time blocking of a 3D plan: `depth` time steps per kernel pass, 1 or 2.
  * At depth 2 one pass of one kernel advances two steps (two launches per
  * pass, run as parallel graph branches: the column tiles that meet an x or y
- * CPML band, and the others). A block stages p_s, p_{s-1} and fact of a
- * 30 x 14 column tile plus a one-node ring through TMA, computes step s+1 on
- * the tile and its ring and step s+2 on the tile, streaming one of `zchunks`
- * chunks of z planes; per node and two steps the fields cost 5 words of HBM
+ * CPML band, and the others). A block of 32 x `rows` threads (rows 8 or 16)
+ * stages p_s, p_{s-1} and fact of a 62 x (rows - 2) column tile plus a
+ * one-node ring through TMA, computes step s+1 on the tile and its ring and
+ * step s+2 on the tile (each thread an x pair of nodes), streaming one of
+ * `zchunks` chunks of z planes; per node and two steps the fields cost 5 words of HBM
  * traffic instead of 8, and the CPML state one read and one write instead of
  * two. Results are bitwise those of depth 1; an odd step count ends with a
  * one-step launch. Depth 2 needs a 3D problem whose sources and receivers are
@@ -172,8 +173,8 @@ int awc_plan_autotune(awc_plan* plan, int64_t steps, float* best_ms_per_step);
  * awc_plan_autotune times depth 2 as well and keeps the faster. No
  * counterpart in the reference, whose forward! advances one step per
  * launch sequence (src/shared/acoustic_3D_xPU.jl:124-167). */
-int awc_plan_set_blocking(awc_plan* plan, int32_t depth, int32_t zchunks);
-int awc_plan_get_blocking(const awc_plan* plan, int32_t* depth, int32_t* zchunks);
+int awc_plan_set_blocking(awc_plan* plan, int32_t depth, int32_t rows, int32_t zchunks);
+int awc_plan_get_blocking(const awc_plan* plan, int32_t* depth, int32_t* rows, int32_t* zchunks);
 /* Kernel launches that a run of nsteps steps from the plan's current step
  * issues (for launch accounting at either depth); -1 on a bad argument. */
 int64_t awc_plan_launch_count(const awc_plan* plan, int64_t nsteps);
