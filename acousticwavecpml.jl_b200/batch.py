@@ -168,3 +168,46 @@ def solve2D_batch(models, shots, *, nt, halo=20, rcoef=0.0001, ppw=10.0, freetop
     finally:
         b.close()
     return [recs.seismograms for _, _, recs in shots]
+
+
+def shard(items, rank, world):
+    """The items rank `rank` of `world` takes: rank, rank + world, ... (shots
+    are independent, so a shot set splits over ranks with no exchange)."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} out of range for world size {world}")
+    return list(items)[rank::world]
+
+
+def solve_sharded(shots, run_shots, group=None):
+    """Runs a shot set over the ranks of a torch.distributed group: each rank
+    calls run_shots(its shard) -> one result per shot (a traces array, say),
+    and every rank gets all results back in the order of `shots` (one
+    all_gather of the per-rank lists). Without an initialised process group
+    it runs every shot locally."""
+    import torch.distributed as dist
+
+    on = dist.is_available() and dist.is_initialized()
+    rank = dist.get_rank(group) if on else 0
+    world = dist.get_world_size(group) if on else 1
+    mine = run_shots(shard(shots, rank, world))
+    if len(mine) != len(shard(shots, rank, world)):
+        raise ValueError("run_shots must return one result per shot")
+    if not on:
+        return list(mine)
+    parts = [None] * world
+    dist.all_gather_object(parts, list(mine), group=group)
+    out = [None] * len(shots)
+    for r in range(world):
+        out[r::world] = parts[r]
+    return out
+
+
+def solve2D_batch_sharded(models, shots, *, nt, group=None, **kw):
+    """solve2D_batch over the ranks of a torch.distributed group (one GPU per
+    rank, the device of the current CUDA context): rank r batches shots
+    r, r + N, ... and every rank's Receivers get all seismograms."""
+    traces = solve_sharded(shots, lambda mine: solve2D_batch(models, mine, nt=nt, **kw) if mine
+                           else [], group)
+    for (_, _, recs), tr in zip(shots, traces):
+        recs.seismograms = tr
+    return traces

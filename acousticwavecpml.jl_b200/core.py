@@ -164,6 +164,24 @@ class Plan:
             nsteps = self.problem.nt
         return int(_lib.lib().awc_plan_launch_count(self._h, int(nsteps)))
 
+    def run_snapshots(self, nsteps, nsave, out=None):
+        """Advances nsteps and returns the fields after every step whose count
+        since the reset is a multiple of nsave, as an array (k, *shape) of
+        float64 (`out`, if given, must hold them: (max_snaps, *shape),
+        C-contiguous over the snapshot index with column-major fields)."""
+        p = self.problem
+        shape = (p.nx, p.ny) if p.ndim == 2 else (p.nx, p.ny, p.nz)
+        n = min(int(nsteps), p.nt - self.step)
+        count = max(0, (self.step + n) // nsave - self.step // nsave)
+        if out is None:
+            out = np.zeros((max(count, 1),) + shape[::-1])
+        got = ctypes.c_int64(0)
+        check(_lib.lib().awc_plan_run_snapshots(self._h, int(nsteps), int(nsave), _ptr(out),
+                                                int(out.shape[0]), ctypes.byref(got)),
+              self.ctx.handle)
+        # each snapshot is a column-major field: view it as (nx, ny[, nz])
+        return [np.asfortranarray(out[j].T) for j in range(got.value)]
+
     def set_wait(self, rounds=4096, round_ns=1000000, withhold=-1):
         """Bounded-wait budget of the two-step kernel's pipeline; `withhold`
         (tests of the timeout path only) makes every block skip one load."""

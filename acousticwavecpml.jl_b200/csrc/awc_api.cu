@@ -232,6 +232,7 @@ struct awc_plan {
   void* traces = nullptr;  // [nt][nrec]
   double* staging = nullptr;
   int64_t staging_len = 0;
+  double* snap_staging = nullptr;  // two unpitched fields for snapshot runs (lazily allocated)
   std::vector<void*> allocs;
   // launch shape of the 3D core kernel: tile rows (4, 8, 16; the tile is
   // 64 x by nodes, 32 x by/2 threads) and z planes per block
@@ -1591,6 +1592,92 @@ int awc_plan_run(awc_plan* P, int64_t nsteps, int32_t use_graph, float* ms) {
 }
 
 int64_t awc_plan_step(const awc_plan* P) { return P ? P->step : -1; }
+
+int awc_plan_run_snapshots(awc_plan* P, int64_t nsteps, int64_t nsave, double* out,
+                           int64_t max_snaps, int64_t* nsnaps) {
+  if (!P) return set_err(nullptr, AWC_ERR_INVALID, "plan is NULL");
+  awc_ctx* C = P->ctx;
+  if (nsnaps) *nsnaps = 0;
+  if (nsteps < 0 || nsave < 1 || max_snaps < 0)
+    return set_err(&C->err, AWC_ERR_INVALID, "nsteps >= 0, nsave >= 1 and max_snaps >= 0 needed");
+  const int64_t n = std::min<int64_t>(nsteps, P->p.nt - P->step);
+  if (n <= 0) return AWC_OK;
+  const int64_t first = P->step, last = P->step + n;  // steps first+1 .. last complete
+  const int64_t count = last / nsave - first / nsave;
+  if (count > max_snaps)
+    return set_err(&C->err, AWC_ERR_INVALID,
+                   "%lld snapshots fall in this run but out holds %lld",
+                   (long long)count, (long long)max_snaps);
+  if (count > 0 && !out) return set_err(&C->err, AWC_ERR_INVALID, "out is NULL");
+  CUDA_TRY(&C->err, cudaSetDevice(C->device));
+  int rc;
+  if ((rc = prepare_launch(P))) return rc;
+  // two device staging slots of N doubles: the unpitched copy of snapshot k
+  // goes to slot k % 2, then to the host on the second stream while the next
+  // steps run
+  if (count > 0 && !P->snap_staging && (rc = P->alloc((void**)&P->snap_staging, 2 * P->N * 8)))
+    return rc;
+  cudaEvent_t ready = nullptr, copied[2] = {nullptr, nullptr};
+  auto cleanup = [&]() {
+    if (ready) cudaEventDestroy(ready);
+    for (cudaEvent_t e : copied)
+      if (e) cudaEventDestroy(e);
+  };
+  if (cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&copied[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&copied[1], cudaEventDisableTiming) != cudaSuccess) {
+    cleanup();
+    return set_err(&C->err, AWC_ERR_CUDA, "event creation failed");
+  }
+  StepState stt = P->state;
+  int64_t it = first, k = 0;
+  bool used[2] = {false, false};
+  const int blocks = grid_for(C, P->N, 256);
+  while (it < last) {
+    const int64_t next = std::min<int64_t>(last, (it / nsave + 1) * nsave);
+    if ((rc = launch_range(P, it, next - it, stt, C->stream))) {
+      cleanup();
+      return rc;
+    }
+    it = next;
+    if (it % nsave != 0) continue;
+    const int slot = (int)(k & 1);
+    double* dst = P->snap_staging + slot * P->N;
+    cudaError_t e = cudaSuccess;
+    if (used[slot]) e = cudaStreamWaitEvent(C->stream, copied[slot], 0);
+    if (e == cudaSuccess) {
+      if (P->p.precision == AWC_F64)
+        awc::unpitch<double><<<blocks, 256, 0, C->stream>>>((const double*)P->buf[stt.ord[0]], dst,
+                                                            P->N, P->p.nx, P->px);
+      else
+        awc::unpitch<float><<<blocks, 256, 0, C->stream>>>((const float*)P->buf[stt.ord[0]], dst,
+                                                           P->N, P->p.nx, P->px);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ready, C->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(C->stream2, ready, 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(out + k * P->N, dst, P->N * 8, cudaMemcpyDeviceToHost, C->stream2);
+    if (e == cudaSuccess) e = cudaEventRecord(copied[slot], C->stream2);
+    if (e != cudaSuccess) {
+      cudaStreamSynchronize(C->stream2);
+      cudaStreamSynchronize(C->stream);
+      cleanup();
+      return set_err(&C->err, AWC_ERR_CUDA, "snapshot copy failed: %s", cudaGetErrorString(e));
+    }
+    used[slot] = true;
+    ++k;
+  }
+  const cudaError_t e1 = cudaStreamSynchronize(C->stream2), e2 = cudaStreamSynchronize(C->stream);
+  cleanup();
+  if (e1 != cudaSuccess || e2 != cudaSuccess)
+    return set_err(&C->err, AWC_ERR_CUDA, "snapshot run failed: %s",
+                   cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+  P->step = last;
+  P->state = stt;
+  if (nsnaps) *nsnaps = k;
+  return check_device_flag(P);
+}
 
 int awc_plan_traces(awc_plan* P, double* traces) {
   if (!P || !traces) return set_err(nullptr, AWC_ERR_INVALID, "plan/traces is NULL");

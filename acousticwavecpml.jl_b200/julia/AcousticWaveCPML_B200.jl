@@ -84,10 +84,62 @@ function packed_coeffs(halo, dt, ds, vel_max, rcoef, f0, freetop)
     return out
 end
 
+# The do_save branch of solve3D (acoustic_3D_xPU.jl:375-379,479-498): the time
+# loop as a plan run with awc_plan_run_snapshots, writing pcur and the
+# reference's metadata to save_dir/{save_name}_it{it}.h5 after every step it
+# with it % nsave == 0 (HDF5.jl, which the reference's package loads too).
+function _run_with_snapshots(ctx, prob, vel, coeffs, possrcs, dt2srctf, posrecs, ls, halo,
+                             nsave, save_name, save_dir)
+    HDF5 = Base.require(Base.PkgId(Base.UUID("f67ccb44-e63f-5c2f-98bd-6dc0ccc4ba2f"), "HDF5"))
+    mkpath(save_dir)
+    plan = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = ccall((:awc_plan_create, LIBAWCPML), Cint,
+               (Ptr{Cvoid}, Ref{AwcProblem}, Ptr{Float64}, Ptr{Float64}, Ptr{Int64},
+                Ptr{Float64}, Ptr{Int64}, Ref{Ptr{Cvoid}}),
+               ctx, prob, vel, coeffs, possrcs, dt2srctf, posrecs, plan)
+    check(rc, ctx)
+    ns = prob.ndim == 3 ? (prob.nx, prob.ny, prob.nz) : (prob.nx, prob.ny)
+    chunk = 8
+    buf = zeros(Float64, ns..., chunk)
+    got = Ref{Int64}(0)
+    try
+        while (step = ccall((:awc_plan_step, LIBAWCPML), Int64, (Ptr{Cvoid},), plan[])) < prob.nt
+            rc = ccall((:awc_plan_run_snapshots, LIBAWCPML), Cint,
+                       (Ptr{Cvoid}, Int64, Int64, Ptr{Float64}, Int64, Ref{Int64}),
+                       plan[], nsave * chunk - step % nsave, nsave, buf, chunk, got)
+            check(rc, ctx)
+            first_it = (step ÷ nsave + 1) * nsave
+            for j = 1:got[]
+                it = first_it + (j - 1) * nsave
+                path = joinpath(save_dir, "$(save_name)_it$(it).h5")
+                isfile(path) && rm(path)
+                HDF5.h5write(path, "lx", ls[1])
+                HDF5.h5write(path, "ly", ls[2])
+                length(ls) == 3 && HDF5.h5write(path, "lz", ls[3])
+                HDF5.h5write(path, "halo", halo)
+                HDF5.h5write(path, "pcur", selectdim(buf, length(ns) + 1, j) |> collect)
+                HDF5.h5write(path, "possrcs", possrcs)
+                HDF5.h5write(path, "posrecs", posrecs)
+            end
+        end
+        traces = zeros(Float64, prob.nt, prob.nrec)
+        pend = zeros(Float64, ns)
+        check(ccall((:awc_plan_traces, LIBAWCPML), Cint, (Ptr{Cvoid}, Ptr{Float64}), plan[],
+                    traces), ctx)
+        check(ccall((:awc_plan_field, LIBAWCPML), Cint, (Ptr{Cvoid}, Ptr{Float64}), plan[],
+                    pend), ctx)
+        return traces, pend
+    finally
+        ccall((:awc_plan_destroy, LIBAWCPML), Cvoid, (Ptr{Cvoid},), plan[])
+    end
+end
+
 function _solve(ls::NTuple{N,Real}, lt::Real, vel::Array{<:Real,N}, srcs::Sources,
                 recs::Receivers; halo::Integer=20, rcoef::Real=0.0001, ppw::Real=10.0,
                 freetop::Bool=true, precision::Symbol=:f64, dt=nothing, nt=nothing,
-                device::Integer=0) where {N}
+                device::Integer=0, do_save::Bool=false, nsave::Integer=5,
+                save_name::String="acoustic3D_xPU",
+                save_dir::String=joinpath("simulations", "tmp")) where {N}
     f0 = srcs.freqdomain
     vel_max = maximum(vel)
     ns = size(vel)
@@ -108,9 +160,16 @@ function _solve(ls::NTuple{N,Real}, lt::Real, vel::Array{<:Real,N}, srcs::Source
     prob = AwcProblem(Int32(N), precision == :f32 ? AWC_F32 : AWC_F64, ns[1], ns[2],
                       N == 3 ? ns[3] : 1, Int32(halo), Int32(freetop), ds[1], ds[2],
                       N == 3 ? ds[3] : 1.0, dt, nt, srcs.n, recs.n)
+    ctx = context(device)
+    if do_save
+        traces, pend = _run_with_snapshots(ctx, prob, Array{Float64}(vel), coeffs, possrcs,
+                                           dt2srctf, posrecs, ls, halo, nsave, save_name,
+                                           save_dir)
+        recs.seismograms = traces
+        return pend
+    end
     traces = zeros(Float64, nt, recs.n)
     pend = zeros(Float64, ns)
-    ctx = context(device)
     rc = ccall((:awc_forward, LIBAWCPML), Cint,
                (Ptr{Cvoid}, Ref{AwcProblem}, Ptr{Float64}, Ptr{Float64}, Ptr{Int64},
                 Ptr{Float64}, Ptr{Int64}, Ptr{Float64}, Ptr{Float64}),
@@ -133,10 +192,12 @@ solve2D(lx::Real, ly::Real, lt::Real, vel::Matrix{<:Real}, srcs::Sources, recs::
 
 """
     solve3D(lx, ly, lz, lt, vel, srcs, recs; halo=20, rcoef=0.0001, ppw=10.0, freetop=true,
-            precision=:f64, dt=nothing, nt=nothing, device=0)
+            precision=:f64, dt=nothing, nt=nothing, device=0, do_save=false, nsave=5,
+            save_name="acoustic3D_xPU", save_dir="simulations/tmp")
 
 `Acoustic3D_CUDA.solve3D` with the time loop on a B200 (depth on the second
-axis, free top at j = 1).
+axis, free top at j = 1). `do_save` writes the reference's HDF5 snapshot
+files (pcur and metadata after every nsave-th step).
 """
 solve3D(lx::Real, ly::Real, lz::Real, lt::Real, vel::Array{<:Real,3}, srcs::Sources,
         recs::Receivers; kw...) = _solve((lx, ly, lz), lt, vel, srcs, recs; kw...)

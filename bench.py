@@ -48,6 +48,9 @@ def parse_args():
                     help="device-resident leg only (no e2e, FP64 or CPU legs); for profiling")
     ap.add_argument("--launch", default=None,
                     help="tile_y,zchunk,band_zchunk of the 3D step instead of autotuning")
+    ap.add_argument("--no-oracle", action="store_true",
+                    help="skip the full-length error check against the FP64 oracle (~1.5 min "
+                         "of host time)")
     ap.add_argument("--blocking", default=None, metavar="DEPTH,ZCHUNKS[,ROWS]",
                     help="fixed time blocking of the 3D leg (default: the autotuner's choice)")
     ap.add_argument("--batch-only", default=None, metavar="TILE_Y,BLOCKS_PER_SM",
@@ -241,7 +244,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def batch_leg(pkg, ctx, args, rank, world, timed, peak):
+def batch_leg(pkg, ctx, args, rank, world, timed, peak, keep=None):
     """Batched 2D shots, FP32: the 96 shots of the six-model layered workload,
     rank r taking shots r, r + N, ... (no data-path collective). One step of
     this leg = every shot of the rank's batch advanced over all nt time steps
@@ -249,7 +252,7 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak):
     from acousticwavecpml_b200 import workloads as W
     w = W.config3()
     shots = W.batch_shots(pkg, w)
-    mine = shots[rank::world]
+    mine = pkg.batch.shard(shots, rank, world)
     probs, vels, setups, idx = pkg.prepare_batch(w["models"], mine, **w["kwargs"])
     b = pkg.Batch(ctx, probs, vels, setups, idx)
     b.autotune(20)
@@ -266,6 +269,13 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak):
     nodes = sum(st["problem"].nx * st["problem"].ny for st in setups)
     t_ts = ms / 1e3 / (k * nt)
     ty, bps = b.get_launch()
+    if keep is not None:  # traces of the first shot of each model (for the oracle check)
+        first = {}
+        for k, sh in enumerate(w["shots"]):
+            first.setdefault(sh["model"], k)
+        for m, k in first.items():
+            if k % world == rank:
+                keep[k] = (w, b.traces(k // world))
     b.close()
     achieved = words * 4 / t_ts / 1e9
     return {"workload": w["name"], "shots": len(shots), "models": len(w["models"]),
@@ -282,6 +292,53 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak):
                                  else "step2d_batch (register strips)"},
             "gpu_launches": k * nt, "timed_runs": k,
             "sharding": f"shots {rank}::{world} per rank" if world > 1 else "one batch"}
+
+
+def oracle_check(pkg, ctx, w2, traces32, traces64, pend64, batch_traces):
+    """Relative L2 errors against the FP64 oracle at full length: config 1
+    (2D, 241 x 241, nt = 1000, FP64 and FP32 through awc_forward), config 2
+    (the headline shot, nt = 2000: the timed FP32 run's traces and the FP64
+    build's traces and final field), config 3 (the first shot of each of the
+    six models of the batched run, nt = 3000, FP32)."""
+    from acousticwavecpml_b200 import workloads as W
+    O = G.load_oracle()
+
+    def rel(a, b):
+        nb = float(np.linalg.norm(b))
+        return float(np.linalg.norm(a - b) / (nb if nb > 0 else 1.0))
+
+    out = {"tolerance": {"f64": 1e-10, "f32_traces": 1e-4}}
+    w1 = W.config1()
+    so = O.setup(w1["lengths"], w1["lt"], w1["vel"], w1["src_pos"], w1["t0s"], w1["f0"],
+                 w1["rec_pos"], **w1["kwargs"])
+    pe_o, tr_o = O.forward(so)
+    srcs, recs = W.sources_receivers(pkg, w1)
+    for prec in ("f64", "f32"):
+        s = pkg.prepare(w1["lengths"], w1["lt"], w1["vel"], srcs, recs, precision=prec,
+                        **w1["kwargs"])
+        p = s["problem"]
+        tr = np.zeros((p.nt, p.nrec), order="F")
+        pe = np.zeros(s["vel"].shape, order="F")
+        ctx.forward(p, s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"], s["posrecs"], tr, pe)
+        out[f"config1_{prec}"] = {"traces": rel(tr, tr_o), "field": rel(pe, pe_o)}
+    so = O.setup(w2["lengths"], w2["lt"], w2["vel"], w2["src_pos"], w2["t0s"], w2["f0"],
+                 w2["rec_pos"], **w2["kwargs"])
+    pe_o, tr_o = O.forward(so)
+    out["config2_f32"] = {"traces": rel(traces32, tr_o)}
+    if traces64 is not None:
+        out["config2_f64"] = {"traces": rel(traces64, tr_o), "field": rel(pend64, pe_o)}
+    for k, (w3, tr) in sorted(batch_traces.items()):
+        sh = w3["shots"][k]
+        kw = w3["kwargs"]
+        lx, ly, vel = w3["models"][sh["model"]]
+        dt = pkg.prepare((lx, ly), None, vel,
+                         pkg.Sources(sh["src_pos"], sh["t0s"], [pkg.rickersource1D], sh["f0"]),
+                         pkg.Receivers(sh["rec_pos"]), **kw)["dt"]
+        so = O.setup((lx, ly), None, vel, sh["src_pos"], sh["t0s"], sh["f0"], sh["rec_pos"],
+                     halo=kw["halo"], rcoef=kw["rcoef"], freetop=True, dt=dt, nt=kw["nt"])
+        _, tr_o = O.forward(so)
+        out[f"config3_model{sh['model']}_shot{k}_f32"] = {"traces": rel(tr, tr_o)}
+    return out
 
 
 def batch_profile_run(args, local):
@@ -504,6 +561,7 @@ def main():
             k64 = max(1, min(args.steps, 3))
             ms64 = timed(shot64, k64)
             tr64 = plan64.traces()
+            pe64 = plan64.field()
             plan64.close()
             t64 = ms64 / 1e3 / (k64 * nt)
             ab64 = a_eff(pkg, p64)
@@ -515,7 +573,8 @@ def main():
                                                        (nrm if nrm > 0 else 1.0))
 
         # ---- batched 2D shots (96 shots over 6 layered models), sharded -----
-        line["batch"] = batch_leg(pkg, ctx, args, rank, world, timed, peak)
+        batch_traces = {}
+        line["batch"] = batch_leg(pkg, ctx, args, rank, world, timed, peak, batch_traces)
 
         # ---- 3D gradient by the discrete adjoint (one shot per rank) -------
         def timed_host(fn):
@@ -532,6 +591,13 @@ def main():
             return t
 
         line["gradient"] = gradient_leg(pkg, ctx, rank, world, timed_host)
+
+        # ---- full-length errors against the FP64 oracle (N=1) -------------
+        if world == 1 and rank == 0 and not args.no_oracle:
+            f64 = args.precision == "f32"
+            line["err_vs_oracle"] = oracle_check(pkg, ctx, w, traces_dev,
+                                                 tr64 if f64 else None, pe64 if f64 else None,
+                                                 batch_traces)
 
         # ---- CPU baseline (rank 0 at N=1 only) ------------------------------
         if world == 1 and rank == 0:

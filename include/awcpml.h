@@ -138,6 +138,20 @@ int awc_plan_reset(awc_plan* plan);
 int awc_plan_run(awc_plan* plan, int64_t nsteps, int32_t use_graph, float* ms);
 /* Steps completed since the last reset. */
 int64_t awc_plan_step(const awc_plan* plan);
+/* Snapshot output, the do_save branch of solve3D (acoustic_3D_xPU.jl:375-379,
+ * 479-498, which writes pcur to an HDF5 file after every step it with
+ * it % nsave == 0): advances `nsteps` steps (clamped to nt) like
+ * awc_plan_run and copies the current field after each step whose 1-based
+ * count since the reset is a multiple of nsave into `out` (host memory,
+ * column-major doubles), snapshot j at out + j*nx*ny*nz, in order. The copy
+ * of a snapshot overlaps the steps that follow it (second stream, two device
+ * staging fields); use pinned host memory for the overlap. Returns
+ * AWC_ERR_INVALID, before running, when more than max_snaps snapshots fall in
+ * the run; *nsnaps (may be NULL) receives the number written. Kernels launch
+ * one by one (no graph). Callers split a long run into pieces whose
+ * snapshots fit their buffer and write each piece out as it returns. */
+int awc_plan_run_snapshots(awc_plan* plan, int64_t nsteps, int64_t nsave, double* out,
+                           int64_t max_snaps, int64_t* nsnaps);
 /* Copies the traces (nt*nrec, column-major; rows not yet reached are zero)
  * and the current field (the latest new pressure, nx*ny*nz) to the host. */
 int awc_plan_traces(awc_plan* plan, double* traces);
