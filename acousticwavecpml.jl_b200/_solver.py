@@ -4,10 +4,12 @@ import os
 
 import numpy as np
 
-from .core import a_eff_words, alloc_words, default_context, prepare, word_bytes
+from .core import _shape, a_eff_words, alloc_words, default_context, prepare, word_bytes
 
 
 def _size_str(problem):
+    if problem.ndim == 1:
+        return f"{problem.nx}"
     if problem.ndim == 2:
         return f"{problem.nx}x{problem.ny}"
     return f"{problem.nx}x{problem.ny}x{problem.nz}"
@@ -18,10 +20,11 @@ def _write_snapshot(path, lengths, halo, pcur, possrcs, posrecs):
     (acoustic_3D_xPU.jl:479-498): lx, ly, lz, halo, pcur, possrcs, posrecs.
     HDF5 (.h5) when h5py is importable, else numpy's .npz with the same
     names."""
-    data = dict(lx=float(lengths[0]), ly=float(lengths[1]), halo=int(halo), pcur=pcur,
-                possrcs=possrcs, posrecs=posrecs)
-    if len(lengths) == 3:
-        data["lz"] = float(lengths[2])
+    data = dict(lx=float(lengths[0]), halo=int(halo), pcur=pcur, possrcs=possrcs,
+                posrecs=posrecs)
+    for name, a in (("ly", 1), ("lz", 2)):
+        if len(lengths) > a:
+            data[name] = float(lengths[a])
     try:
         import h5py
     except ImportError:
@@ -50,8 +53,7 @@ def _run_with_snapshots(ctx, s, lengths, halo, nsave, save_name, save_dir, chunk
     try:
         if p.ndim == 3 and p.nt >= 100:
             plan.autotune(10)
-        shape = (p.nx, p.ny) if p.ndim == 2 else (p.nx, p.ny, p.nz)
-        buf = np.zeros((chunk_snaps,) + shape[::-1])
+        buf = np.zeros((chunk_snaps,) + _shape(p)[::-1])
         while plan.step < p.nt:
             start = plan.step
             snaps = plan.run_snapshots(nsave * chunk_snaps - start % nsave, nsave, buf)
@@ -98,7 +100,7 @@ def solve(lengths, lt, vel, srcs, recs, *, halo, rcoef, ppw, freetop, do_bench, 
               f"memory = {alloc_words(p) * wb / 1e9:1.3f} GB")
         return None
     traces = np.zeros((p.nt, p.nrec), order="F")
-    pfinal = np.zeros(s["vel"].shape, order="F")
+    pfinal = np.zeros(_shape(p), order="F")
     ctx.forward(p, s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"], s["posrecs"], traces,
                 pfinal)
     if verbose and p.nt > 0:

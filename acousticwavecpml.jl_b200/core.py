@@ -19,6 +19,11 @@ from ._lib import AWC_F32, AWC_F64, Problem, check
 PRECISIONS = {"f32": AWC_F32, "float32": AWC_F32, "f64": AWC_F64, "float64": AWC_F64}
 
 
+def _shape(p):
+    """Array shape of a problem's fields: (nx,), (nx, ny) or (nx, ny, nz)."""
+    return ((p.nx,), (p.nx, p.ny), (p.nx, p.ny, p.nz))[p.ndim - 1]
+
+
 def _ptr(a):
     """Host address of a numpy array or a torch tensor (None -> NULL)."""
     if a is None:
@@ -170,7 +175,7 @@ class Plan:
         float64 (`out`, if given, must hold them: (max_snaps, *shape),
         C-contiguous over the snapshot index with column-major fields)."""
         p = self.problem
-        shape = (p.nx, p.ny) if p.ndim == 2 else (p.nx, p.ny, p.nz)
+        shape = _shape(p)
         n = min(int(nsteps), p.nt - self.step)
         count = max(0, (self.step + n) // nsave - self.step // nsave)
         if out is None:
@@ -205,7 +210,7 @@ class Plan:
 
     def field(self, out=None):
         p = self.problem
-        shape = (p.nx, p.ny) if p.ndim == 2 else (p.nx, p.ny, p.nz)
+        shape = _shape(p)
         if out is None:
             out = np.zeros(shape, order="F")
         check(_lib.lib().awc_plan_field(self._h, _ptr(out)), self.ctx.handle)
@@ -240,15 +245,19 @@ def problem_coeffs(problem, rcoef, f0, vel_max):
 
 def prepare(lengths, lt, vel, srcs, recs, halo=20, rcoef=0.0001, ppw=10.0, freetop=True,
             precision="f64", dt=None, nt=None):
-    """Host setup of solve2D/solve3D. Returns a dict of the awc_forward inputs.
+    """Host setup of solve1D/solve2D/solve3D. Returns a dict of the awc_forward
+    inputs.
 
     dt/nt default to the reference's rule (dt = sqrt(ndim) / (vmax Σ 1/d_i) / 2,
-    nt = ceil(lt/dt)); passing them fixes the step explicitly instead.
+    which is dx / vmax / 2 in 1D (acoustic_1D.jl); nt = ceil(lt/dt)); passing
+    them fixes the step explicitly instead. 1D has no free top.
     """
     vel = np.asfortranarray(vel, dtype=np.float64)
     ndim = vel.ndim
-    if ndim not in (2, 3) or len(lengths) != ndim:
-        raise ValueError("vel must be 2D or 3D and match the number of model lengths")
+    if ndim not in (1, 2, 3) or len(lengths) != ndim:
+        raise ValueError("vel must be 1D, 2D or 3D and match the number of model lengths")
+    if ndim == 1:
+        freetop = False
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
     shape = vel.shape
@@ -280,11 +289,11 @@ def prepare(lengths, lt, vel, srcs, recs, halo=20, rcoef=0.0001, ppw=10.0, freet
 
     possrcs = snap(srcs.positions, "source")
     posrecs = snap(recs.positions, "receiver")
-    problem = Problem(ndim=ndim, precision=PRECISIONS[precision], nx=shape[0], ny=shape[1],
-                      nz=shape[2] if ndim == 3 else 1, halo=int(halo),
-                      freetop=1 if freetop else 0, dx=d[0], dy=d[1],
-                      dz=d[2] if ndim == 3 else 1.0, dt=float(dt), nt=int(nt),
-                      nsrc=srcs.n, nrec=recs.n)
+    problem = Problem(ndim=ndim, precision=PRECISIONS[precision], nx=shape[0],
+                      ny=shape[1] if ndim >= 2 else 1, nz=shape[2] if ndim == 3 else 1,
+                      halo=int(halo), freetop=1 if freetop else 0, dx=d[0],
+                      dy=d[1] if ndim >= 2 else 1.0, dz=d[2] if ndim == 3 else 1.0,
+                      dt=float(dt), nt=int(nt), nsrc=srcs.n, nrec=recs.n)
     coeffs = problem_coeffs(problem, rcoef, f0, vel_max)
     return dict(problem=problem, vel=vel, coeffs=coeffs, possrcs=possrcs, dt2srctf=dt2srctf,
                 posrecs=posrecs, dt=float(dt), nt=int(nt), d=d, vel_max=vel_max, f0=f0)
@@ -295,6 +304,8 @@ def a_eff_words(problem):
     (acoustic_3D_xPU.jl:520-528, acoustic_2D_xPU.jl:422-428)."""
     h = problem.halo
     nx, ny = problem.nx, problem.ny
+    if problem.ndim == 1:  # acoustic_1D.jl's count
+        return 2 * (4 * (h + 1) + (h + 1)) + 2 * (4 * (h + 1) + (h + 1)) + (4 * nx + nx)
     if problem.ndim == 2:
         return ((h + 1) * ny * 2 * 3 + (h + 1) * nx * 2 * 3 + (h + 1) * ny * 2 * 2 +
                 (h + 1) * nx * 2 * 2 + 4 * nx * ny)
@@ -308,6 +319,8 @@ def alloc_words(problem):
     """The reference's allocated-memory word count (acoustic_3D_xPU.jl:512-518)."""
     h = problem.halo
     nx, ny = problem.nx, problem.ny
+    if problem.ndim == 1:  # acoustic_1D.jl's count
+        return 3 * nx + 2 * (h + 1) + 2 * h + 4 * (h + 1) + 4 * h
     if problem.ndim == 2:
         return (3 * nx * ny + 2 * (h + 1) * ny + 2 * h * ny + 2 * (h + 1) * nx + 2 * h * nx +
                 4 * 2 * (h + 1) + 4 * 2 * h)

@@ -24,7 +24,13 @@
 //   μ_{t+1}[e]   = bKh_e μ_{t+2}[e] + (w_e - w_{e+1}) / d,
 //     w_q = a_{q-1} ν_{t+1}[q-1] + F(c_q) λ_{t+1}(c_q) (0 outside q = 1..h),
 // and dJ/dF(c) = Σ_t λ_{t+1}(c) B_t(c), where B_t is the bracket multiplying
-// F, B_t = (p_{t+1} - 2 p_t + p_{t-1} - S_t)(c) / F(c). Rim nodes carry no
+// F. At a node outside every active CPML band that bracket is the Laplacian
+// of p_t, Σ_axes D2 p_t(c), evaluated from the stored p_t in double; inside
+// a band it also holds the ψ and ξ terms, and B_t = (p_{t+1} - 2 p_t + p_{t-1}
+// - S_t)(c) / F(c) there. (The difference form divides a second difference
+// in time, about (ω dt)² ≈ 1e-3 of p, by F, and at a source node subtracts
+// the injected value from it: in FP32 its rounding error dominates the
+// gradient near sources, which the Laplacian form avoids.) Rim nodes carry no
 // adjoint: their values never depend on the interior or on c². Sides whose
 // recursion is trivial (the free top) feed nothing back and are skipped, as
 // in the forward. Bands must not overlap (n >= 2 halo + 2 on every axis with
@@ -141,10 +147,24 @@ __global__ void adj_residuals(T* __restrict__ lam3, const int64_t* __restrict__ 
   lam3[node[n]] = v;
 }
 
+// Whether node (i, j, k) lies in an active CPML band of any axis (where the
+// forward bracket holds ψ/ξ terms besides the Laplacian).
+template <typename T>
+__device__ __forceinline__ bool adj_in_band(const AdjParams<T>& A, int i, int j, int k) {
+  if (A.halo == 0) return false;
+  const int c[3] = {i, j, k}, n[3] = {A.nx, A.ny, A.nz};
+  for (int a = 0; a < A.ndim; ++a)
+    if ((A.active[a][0] && c[a] <= A.halo) || (A.active[a][1] && c[a] >= n[a] - A.halo - 1))
+      return true;
+  return false;
+}
+
 // λ_{t+1} = 2 λ_{t+2} - λ_{t+3} (residuals included, see adj_residuals) plus
 // the transposed stencil of G = F λ_{t+2} and the band terms, one thread per
-// node; then at the same node G = F λ_{t+1} for the next step and the gradient accumulation dJ/dF += λ_{t+1} (p_{t+1} - 2 p_t +
-// p_{t-1}) / F (the source term is removed by adj_sources).
+// node; then at the same node G = F λ_{t+1} for the next step and the
+// gradient accumulation dJ/dF += λ_{t+1} B_t: the Laplacian of p_t outside
+// the bands, (p_{t+1} - 2 p_t + p_{t-1}) / F inside them (where adj_sources
+// removes the source term).
 template <typename T>
 __global__ void __launch_bounds__(256) adj_lambda_grad(AdjParams<T> A, T* __restrict__ Gn,
                                                        const T* __restrict__ pm1,
@@ -171,8 +191,18 @@ __global__ void __launch_bounds__(256) adj_lambda_grad(AdjParams<T> A, T* __rest
   const T f = __ldg(A.F + o);
   Gn[o] = f * lam;
   if (grad) {
-    const double b = ((double)__ldg(pp1 + o) - 2.0 * (double)__ldg(p0 + o) +
-                      (double)__ldg(pm1 + o)) / (double)f;
+    double b;
+    if (adj_in_band(A, i, j, k)) {
+      b = ((double)__ldg(pp1 + o) - 2.0 * (double)__ldg(p0 + o) + (double)__ldg(pm1 + o)) /
+          (double)f;
+    } else {
+      const double c = __ldg(p0 + o);
+      b = (double)A.inv_d2[0] * (((double)__ldg(p0 + o + 1) - 2.0 * c) + (double)__ldg(p0 + o - 1)) +
+          (double)A.inv_d2[1] * (((double)__ldg(p0 + o + px) - 2.0 * c) + (double)__ldg(p0 + o - px));
+      if (A.ndim == 3)
+        b += (double)A.inv_d2[2] *
+             (((double)__ldg(p0 + o + plane) - 2.0 * c) + (double)__ldg(p0 + o - plane));
+    }
     grad[o] += (double)lam * b;
   }
 }
@@ -244,15 +274,16 @@ __global__ void __launch_bounds__(256) adj_band(AdjParams<T> A, AdjSides L) {
 // removal of the source term from the gradient bracket.
 template <typename T>
 __global__ void adj_sources(const T* __restrict__ lamn, const T* __restrict__ F,
-                            const int64_t* __restrict__ node, int32_t nsrc,
-                            const T* __restrict__ stf_row, double* __restrict__ grad,
-                            T* __restrict__ out_row) {
+                            const int64_t* __restrict__ node, const int8_t* __restrict__ in_band,
+                            int32_t nsrc, const T* __restrict__ stf_row,
+                            double* __restrict__ grad, T* __restrict__ out_row) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int s = 0; s < nsrc; ++s) {
     const int64_t o = node[s];
     if (o < 0) continue;  // rim source: no adjoint
     if (out_row) out_row[s] = lamn[o];
-    if (grad) grad[o] -= (double)lamn[o] * (double)stf_row[s] / (double)F[o];
+    // only band nodes use the difference form of the bracket, which holds S_t
+    if (grad && in_band[s]) grad[o] -= (double)lamn[o] * (double)stf_row[s] / (double)F[o];
   }
 }
 
@@ -404,6 +435,21 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
   ADJ_TRY(C, cudaMemcpyAsync(roff_d, RG.off.data(), RG.off.size() * 4, cudaMemcpyHostToDevice, st));
   if (!snode.empty())
     ADJ_TRY(C, cudaMemcpyAsync(snode_d, snode.data(), snode.size() * 8, cudaMemcpyHostToDevice, st));
+  // which sources sit in an active CPML band (their bracket uses S_t)
+  std::vector<int8_t> sband(std::max<int64_t>(nsrc, 1), 0);
+  {
+    const int64_t nn[3] = {p->nx, p->ny, V.nz};
+    for (int64_t s2 = 0; s2 < nsrc; ++s2) {
+      const int64_t c[3] = {possrcs[s2] - 1, possrcs[s2 + nsrc] - 1,
+                            p->ndim == 3 ? possrcs[s2 + 2 * nsrc] - 1 : 0};
+      for (int a = 0; a < p->ndim && h > 0; ++a)
+        if ((V.active[a][0] && c[a] <= h) || (V.active[a][1] && c[a] >= nn[a] - h - 1))
+          sband[s2] = 1;
+    }
+  }
+  int8_t* sband_d;
+  ADJ_TRY(C, mem.get(&sband_d, sband.size()));
+  ADJ_TRY(C, cudaMemcpyAsync(sband_d, sband.data(), sband.size(), cudaMemcpyHostToDevice, st));
   // kernel parameters
   awc::AdjParams<T> A{};
   A.ndim = p->ndim;
@@ -547,8 +593,9 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       const T* pp1 = want_grad ? seg[t - s + 2] : nullptr;
       awc::adj_lambda_grad<T><<<grid, blk, 0, st>>>(A, G[gi ^ 1], pm1, p0, pp1, grad);
       if (nsrc > 0)
-        awc::adj_sources<T><<<1, 32, 0, st>>>(ln, A.F, snode_d, (int32_t)nsrc, stf_d + t * nsrc,
-                                              grad, sout_d ? sout_d + t * nsrc : nullptr);
+        awc::adj_sources<T><<<1, 32, 0, st>>>(ln, A.F, snode_d, sband_d, (int32_t)nsrc,
+                                              stf_d + t * nsrc, grad,
+                                              sout_d ? sout_d + t * nsrc : nullptr);
       if (sides.n > 0) awc::adj_band<T><<<band_blocks, 256, 0, st>>>(A, sides);
       ADJ_TRY(C, cudaGetLastError());
       std::swap(i2, i3);  // λ_{t+1} is the next step's λ_{t+2}
@@ -584,6 +631,8 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
 
 int check_adjoint_problem(awc_ctx* C, const awc_problem* p) {
   if (!p) return awc::fail(C, AWC_ERR_INVALID, "problem is NULL");
+  if (p->ndim != 2 && p->ndim != 3)
+    return awc::fail(C, AWC_ERR_INVALID, "the adjoint solves 2D and 3D problems");
   const int64_t n[3] = {p->nx, p->ny, p->ndim == 3 ? p->nz : 1};
   for (int a = 0; a < p->ndim; ++a)
     if (p->halo > 0 && n[a] < 2 * (int64_t)p->halo + 2)

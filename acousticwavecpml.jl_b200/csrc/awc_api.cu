@@ -87,7 +87,9 @@ void kab(int32_t halo, double dt, double npower, double d0, double alpha_max, do
   }
 }
 
-int validate(const awc_problem* p, std::string* err) {
+// lifted1d: p is the three-row form of a 1D problem, whose y axis carries no
+// CPML (its halo is not bounded by ny).
+int validate(const awc_problem* p, std::string* err, bool lifted1d = false) {
   if (!p) return set_err(err, AWC_ERR_INVALID, "problem is NULL");
   if (p->ndim != 2 && p->ndim != 3)
     return set_err(err, AWC_ERR_INVALID, "ndim must be 2 or 3 (got %d)", p->ndim);
@@ -101,6 +103,7 @@ int validate(const awc_problem* p, std::string* err) {
   if (p->ndim == 2 && p->nz != 1) return set_err(err, AWC_ERR_INVALID, "2D problems need nz = 1");
   if (p->halo < 0) return set_err(err, AWC_ERR_INVALID, "halo must be >= 0");
   for (int a = 0; a < p->ndim; ++a) {
+    if (lifted1d && a == 1) continue;
     // right-band ψ reads pcur[i + n - halo - 2] for i = 1 (acoustic_3D_xPU.jl:12)
     if (p->halo > n[a] - 2)
       return set_err(err, AWC_ERR_INVALID, "halo %d too large for %lld nodes on axis %d",
@@ -130,6 +133,52 @@ int check_positions(const awc_problem* p, const int64_t* pos, int64_t cnt, const
         return set_err(err, AWC_ERR_INVALID, "At least one %s is not inside the model!", what);
     }
   return AWC_OK;
+}
+
+// A 1D problem (the reference's solve1D, src/shared/acoustic_1D.jl:7-89)
+// runs as the 2D problem of three rows whose middle row is the line: the
+// outer rows are Dirichlet rim (never updated, zero), the y spacing enters
+// with zero inverse (plan flag is1d), and the y CPML block is the trivial
+// one (a = 0, b/K = 1), so every node of the line takes exactly the 1D
+// update: pnew = 2 pcur - pold + fact (d2x + 0) + damp_x.
+struct Lifted {
+  awc_problem p{};
+  std::vector<double> vel, coeffs;
+  std::vector<int64_t> possrcs, posrecs;
+};
+
+int validate_1d(const awc_problem* p, std::string* err) {
+  if (p->ny != 1 || p->nz != 1) return set_err(err, AWC_ERR_INVALID, "1D problems need ny = nz = 1");
+  awc_problem q = *p;
+  q.ndim = 2;
+  q.ny = 3;
+  q.dy = p->dx;
+  return validate(&q, err, true);
+}
+
+void lift_1d(const awc_problem* p, const double* vel, const double* coeffs, const int64_t* possrcs,
+             const int64_t* posrecs, Lifted* L) {
+  const int64_t nx = p->nx, h = p->halo;
+  L->p = *p;
+  L->p.ndim = 2;
+  L->p.ny = 3;
+  L->p.nz = 1;
+  L->p.dy = p->dx;  // its inverse is replaced by 0 (awc_plan.is1d)
+  L->p.freetop = 0;
+  L->vel.assign(3 * nx, 0.0);
+  for (int r = 0; r < 3; ++r)
+    for (int64_t i = 0; i < nx; ++i) L->vel[i + nx * r] = vel ? vel[i] : 0.0;
+  L->coeffs.assign(2 * (8 * h + 4), 0.0);
+  if (coeffs) std::copy(coeffs, coeffs + 8 * h + 4, L->coeffs.begin());
+  double* yb = L->coeffs.data() + 8 * h + 4;  // y block: a = 0, b/K = 1
+  for (int64_t m = 0; m < 2 * h; ++m) yb[2 * h + m] = 1.0;
+  for (int64_t m = 0; m < 2 * (h + 1); ++m) yb[4 * h + 2 * (h + 1) + m] = 1.0;
+  auto lift_pos = [](const int64_t* pos, int64_t n, std::vector<int64_t>& out) {
+    out.assign(2 * std::max<int64_t>(n, 1), 2);
+    for (int64_t s = 0; s < n; ++s) out[s] = pos ? pos[s] : 0;
+  };
+  lift_pos(possrcs, p->nsrc, L->possrcs);
+  lift_pos(posrecs, p->nrec, L->posrecs);
 }
 
 // Row pitch of the field arrays: nx rounded up to 32 elements.
@@ -252,6 +301,7 @@ struct awc_plan {
   CUtensorMap tb_map_pt[4], tb_map_in[4], tb_map_f;
   int32_t tb_maps_rows = 0;  // rows the tensor maps were encoded for
   int32_t wait_rounds = 4096, wait_ns = 1000000, withhold = -1;
+  bool is1d = false;  // a 1D problem lifted to three rows (see Lifted)
   // run state
   int64_t step = 0;
   StepState state;
@@ -538,6 +588,7 @@ awc::StepParams<T> step_params(const awc_plan* P, int64_t it, const StepState& s
     S.inv_d[a] = (T)(1.0 / d[a]);
     S.inv_d2[a] = (T)(1.0 / (d[a] * d[a]));
   }
+  if (P->is1d) S.inv_d[1] = S.inv_d2[1] = T(0);  // no y derivative on the line
   const int64_t h = p->halo;
   const T* cf = (const T*)P->coef;
   for (int a = 0; a < p->ndim; ++a) {
@@ -1279,10 +1330,10 @@ void default_tuning(awc_plan* P) {
 
 int forward_impl(awc_ctx* C, const awc_problem* p, const double* vel, const double* coeffs,
                  const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
-                 awc_plan** out) {
+                 awc_plan** out, bool lifted1d = false) {
   std::string* err = &C->err;
   int rc;
-  if ((rc = validate(p, err))) return rc;
+  if ((rc = validate(p, err, lifted1d))) return rc;
   if (!vel || !coeffs) return set_err(err, AWC_ERR_INVALID, "vel/coeffs are NULL");
   if (p->nsrc > 0 && p->nt > 0 && !dt2srctf)
     return set_err(err, AWC_ERR_INVALID, "dt2srctf is NULL");
@@ -1394,7 +1445,7 @@ void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t coun
 extern "C" {
 
 int64_t awc_coeffs_len(const awc_problem* p) {
-  if (!p || (p->ndim != 2 && p->ndim != 3) || p->halo < 0) return 0;
+  if (!p || p->ndim < 1 || p->ndim > 3 || p->halo < 0) return 0;
   return (int64_t)p->ndim * (8 * (int64_t)p->halo + 4);
 }
 
@@ -1410,7 +1461,7 @@ int awc_cpml_coeffs(int32_t halo, double dt, double npower, double d0, double al
 
 int awc_problem_coeffs(const awc_problem* p, double rcoef, double f0, double vel_max,
                        double* coeffs) {
-  int rc = validate(p, nullptr);
+  int rc = p && p->ndim == 1 ? validate_1d(p, nullptr) : validate(p, nullptr);
   if (rc) return rc;
   if (!coeffs) return set_err(nullptr, AWC_ERR_INVALID, "coeffs is NULL");
   const int64_t h = p->halo;
@@ -1516,6 +1567,21 @@ int awc_plan_create(awc_ctx* ctx, const awc_problem* p, const double* vel, const
                     awc_plan** out) {
   if (!ctx || !out) return set_err(nullptr, AWC_ERR_INVALID, "ctx/out is NULL");
   *out = nullptr;
+  if (p && p->ndim == 1) {
+    int rc;
+    if ((rc = validate_1d(p, &ctx->err)) ||
+        (rc = check_positions(p, possrcs, p->nsrc, "source", &ctx->err)) ||
+        (rc = check_positions(p, posrecs, p->nrec, "receiver", &ctx->err)))
+      return rc;
+    if (!vel || !coeffs) return set_err(&ctx->err, AWC_ERR_INVALID, "vel/coeffs are NULL");
+    Lifted L;
+    lift_1d(p, vel, coeffs, possrcs, posrecs, &L);
+    if ((rc = forward_impl(ctx, &L.p, L.vel.data(), L.coeffs.data(), L.possrcs.data(), dt2srctf,
+                           L.posrecs.data(), out, true)))
+      return rc;
+    (*out)->is1d = true;
+    return AWC_OK;
+  }
   return forward_impl(ctx, p, vel, coeffs, possrcs, dt2srctf, posrecs, out);
 }
 
@@ -1642,22 +1708,25 @@ int awc_plan_run_snapshots(awc_plan* P, int64_t nsteps, int64_t nsave, double* o
     it = next;
     if (it % nsave != 0) continue;
     const int slot = (int)(k & 1);
+    const int64_t nf = P->is1d ? P->p.nx : P->N;  // values per snapshot
     double* dst = P->snap_staging + slot * P->N;
+    const size_t row = P->is1d ? (size_t)P->px * P->esz : 0;  // a 1D plan's line is row 1
     cudaError_t e = cudaSuccess;
     if (used[slot]) e = cudaStreamWaitEvent(C->stream, copied[slot], 0);
     if (e == cudaSuccess) {
+      const char* src = (const char*)P->buf[stt.ord[0]] + row;
       if (P->p.precision == AWC_F64)
-        awc::unpitch<double><<<blocks, 256, 0, C->stream>>>((const double*)P->buf[stt.ord[0]], dst,
-                                                            P->N, P->p.nx, P->px);
+        awc::unpitch<double><<<blocks, 256, 0, C->stream>>>((const double*)src, dst, nf,
+                                                            P->p.nx, P->px);
       else
-        awc::unpitch<float><<<blocks, 256, 0, C->stream>>>((const float*)P->buf[stt.ord[0]], dst,
-                                                           P->N, P->p.nx, P->px);
+        awc::unpitch<float><<<blocks, 256, 0, C->stream>>>((const float*)src, dst, nf, P->p.nx,
+                                                           P->px);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaEventRecord(ready, C->stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(C->stream2, ready, 0);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(out + k * P->N, dst, P->N * 8, cudaMemcpyDeviceToHost, C->stream2);
+      e = cudaMemcpyAsync(out + k * nf, dst, nf * 8, cudaMemcpyDeviceToHost, C->stream2);
     if (e == cudaSuccess) e = cudaEventRecord(copied[slot], C->stream2);
     if (e != cudaSuccess) {
       cudaStreamSynchronize(C->stream2);
@@ -1700,15 +1769,16 @@ int awc_plan_field(awc_plan* P, double* out) {
   if (!P || !out) return set_err(nullptr, AWC_ERR_INVALID, "plan/out is NULL");
   awc_ctx* C = P->ctx;
   CUDA_TRY(&C->err, cudaSetDevice(C->device));
-  // the latest new field (the reference's pcur)
-  const void* cur = P->buf[P->state.ord[0]];
-  const int blocks = grid_for(C, P->N, 256);
+  // the latest new field (the reference's pcur); a 1D plan's line is row 1
+  const int64_t n = P->is1d ? P->p.nx : P->N;
+  const char* cur = (const char*)P->buf[P->state.ord[0]] + (P->is1d ? P->px * P->esz : 0);
+  const int blocks = grid_for(C, n, 256);
   if (P->p.precision == AWC_F64)
-    awc::unpitch<double><<<blocks, 256, 0, C->stream>>>((const double*)cur, P->staging, P->N, P->p.nx, P->px);
+    awc::unpitch<double><<<blocks, 256, 0, C->stream>>>((const double*)cur, P->staging, n, P->p.nx, P->px);
   else
-    awc::unpitch<float><<<blocks, 256, 0, C->stream>>>((const float*)cur, P->staging, P->N, P->p.nx, P->px);
+    awc::unpitch<float><<<blocks, 256, 0, C->stream>>>((const float*)cur, P->staging, n, P->p.nx, P->px);
   CUDA_TRY(&C->err, cudaGetLastError());
-  CUDA_TRY(&C->err, cudaMemcpyAsync(out, P->staging, P->N * 8, cudaMemcpyDeviceToHost, C->stream));
+  CUDA_TRY(&C->err, cudaMemcpyAsync(out, P->staging, n * 8, cudaMemcpyDeviceToHost, C->stream));
   CUDA_TRY(&C->err, cudaStreamSynchronize(C->stream));
   return AWC_OK;
 }
@@ -1892,6 +1962,21 @@ int awc_forward(awc_ctx* ctx, const awc_problem* p, const double* vel, const dou
                 const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
                 double* traces, double* pfinal) {
   if (!ctx) return set_err(nullptr, AWC_ERR_INVALID, "ctx is NULL");
+  if (p && p->ndim == 1) {
+    int rc;
+    if ((rc = validate_1d(p, &ctx->err)) ||
+        (rc = check_positions(p, possrcs, p->nsrc, "source", &ctx->err)) ||
+        (rc = check_positions(p, posrecs, p->nrec, "receiver", &ctx->err)))
+      return rc;
+    if (!vel || !coeffs) return set_err(&ctx->err, AWC_ERR_INVALID, "vel/coeffs are NULL");
+    awc_plan* P = nullptr;
+    if ((rc = awc_plan_create(ctx, p, vel, coeffs, possrcs, dt2srctf, posrecs, &P))) return rc;
+    rc = awc_plan_run(P, p->nt, 1, &ctx->last_run_ms);
+    if (!rc && traces) rc = awc_plan_traces(P, traces);
+    if (!rc && pfinal) rc = awc_plan_field(P, pfinal);
+    awc_plan_destroy(P);
+    return rc;
+  }
   int rc = validate(p, &ctx->err);
   if (rc) return rc;
   if (p->nt * p->nrec > 0 && !traces) return set_err(&ctx->err, AWC_ERR_INVALID, "traces is NULL");

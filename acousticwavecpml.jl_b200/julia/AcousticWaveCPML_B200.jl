@@ -21,7 +21,7 @@ module AcousticWaveCPML_B200
 
 import ..AcousticWaveCPML: Sources, Receivers, calc_Kab_CPML
 
-export solve2D, solve3D, misfit, misfit_gradient
+export solve1D, solve2D, solve3D, misfit, misfit_gradient
 
 const LIBAWCPML = get(ENV, "AWCPML_LIB", joinpath(@__DIR__, "..", "lib", "libawcpml.so"))
 
@@ -157,9 +157,9 @@ function _solve(ls::NTuple{N,Real}, lt::Real, vel::Array{<:Real,N}, srcs::Source
     @assert all(all(1 .<= possrcs[:, a] .<= ns[a]) for a in 1:N) "At least one source is not inside the model!"
     @assert all(all(1 .<= posrecs[:, a] .<= ns[a]) for a in 1:N) "At least one receiver is not inside the model!"
     coeffs = packed_coeffs(halo, dt, ds, vel_max, rcoef, f0, freetop)
-    prob = AwcProblem(Int32(N), precision == :f32 ? AWC_F32 : AWC_F64, ns[1], ns[2],
-                      N == 3 ? ns[3] : 1, Int32(halo), Int32(freetop), ds[1], ds[2],
-                      N == 3 ? ds[3] : 1.0, dt, nt, srcs.n, recs.n)
+    prob = AwcProblem(Int32(N), precision == :f32 ? AWC_F32 : AWC_F64, ns[1],
+                      N >= 2 ? ns[2] : 1, N == 3 ? ns[3] : 1, Int32(halo), Int32(freetop),
+                      ds[1], N >= 2 ? ds[2] : 1.0, N == 3 ? ds[3] : 1.0, dt, nt, srcs.n, recs.n)
     ctx = context(device)
     if do_save
         traces, pend = _run_with_snapshots(ctx, prob, Array{Float64}(vel), coeffs, possrcs,
@@ -189,6 +189,16 @@ production single-precision build; `dt`/`nt` fix the time step explicitly.
 """
 solve2D(lx::Real, ly::Real, lt::Real, vel::Matrix{<:Real}, srcs::Sources, recs::Receivers; kw...) =
     _solve((lx, ly), lt, vel, srcs, recs; kw...)
+
+"""
+    solve1D(lx, lt, vel, srcs, recs; halo=20, rcoef=0.0001, ppw=10.0, precision=:f64,
+            dt=nothing, nt=nothing, device=0)
+
+`Acoustic1D.solve1D` (src/shared/acoustic_1D.jl:89-297) with the time loop on
+a B200 (awc_forward with ndim = 1; no free top in 1D).
+"""
+solve1D(lx::Real, lt::Real, vel::Vector{<:Real}, srcs::Sources, recs::Receivers; kw...) =
+    _solve((lx,), lt, vel, srcs, recs; freetop=false, kw...)
 
 """
     solve3D(lx, ly, lz, lt, vel, srcs, recs; halo=20, rcoef=0.0001, ppw=10.0, freetop=true,

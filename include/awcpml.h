@@ -43,9 +43,14 @@ extern "C" {
 #define AWC_F64 2 /* everything in double (parity build) */
 
 /* One forward problem: a single shot on one velocity model.
- * Mirrors the scalars solve2D/solve3D derive (acoustic_3D_xPU.jl:195-206). */
+ * Mirrors the scalars solve2D/solve3D derive (acoustic_3D_xPU.jl:195-206),
+ * and solve1D's (src/shared/acoustic_1D.jl:104-128) with ndim = 1:
+ * ny = nz = 1, dy/dz/freetop unused, positions (n x 1); a 1D problem runs as
+ * the middle line of a three-row 2D problem with no y derivative and no y
+ * CPML (awc_forward, the plan API and snapshots; not the batch, adjoint or
+ * learned-layer entry points). */
 typedef struct awc_problem {
-  int32_t ndim;      /* 2 or 3 */
+  int32_t ndim;      /* 1, 2 or 3 */
   int32_t precision; /* AWC_F32 or AWC_F64 */
   int64_t nx, ny, nz;
   int32_t halo;    /* CPML layers per side (reference keyword `halo`) */

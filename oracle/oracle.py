@@ -130,7 +130,9 @@ def setup(lengths, lt, vel, src_positions, t0s, f0, rec_positions, halo=20, rcoe
     """
     vel = np.asfortranarray(vel, dtype=np.float64)
     ndim = vel.ndim
-    assert ndim in (2, 3) and len(lengths) == ndim
+    assert ndim in (1, 2, 3) and len(lengths) == ndim
+    if ndim == 1:
+        freetop = False  # acoustic_1D.jl has no free top
     shape = vel.shape
     vel_max = float(vel.max())
     d = [lengths[a] / (shape[a] - 1) for a in range(ndim)]
@@ -160,10 +162,10 @@ def setup(lengths, lt, vel, src_positions, t0s, f0, rec_positions, halo=20, rcoe
         return out
 
     possrcs, posrecs = snap(src_positions), snap(rec_positions)
-    p = Problem(ndim=ndim, precision=2, nx=shape[0], ny=shape[1],
+    p = Problem(ndim=ndim, precision=2, nx=shape[0], ny=shape[1] if ndim >= 2 else 1,
                 nz=shape[2] if ndim == 3 else 1, halo=halo, freetop=1 if freetop else 0,
-                dx=d[0], dy=d[1], dz=d[2] if ndim == 3 else 1.0, dt=dt, nt=nt,
-                nsrc=nsrc, nrec=nrec)
+                dx=d[0], dy=d[1] if ndim >= 2 else 1.0, dz=d[2] if ndim == 3 else 1.0, dt=dt,
+                nt=nt, nsrc=nsrc, nrec=nrec)
     coeffs = problem_coeffs(p, rcoef, f0, vel_max)
     return dict(problem=p, vel=vel, coeffs=coeffs, possrcs=np.asfortranarray(possrcs),
                 dt2srctf=dt2srctf, posrecs=np.asfortranarray(posrecs), dt=dt, nt=nt,
@@ -173,6 +175,14 @@ def setup(lengths, lt, vel, src_positions, t0s, f0, rec_positions, halo=20, rcoe
 def problem_coeffs(p, rcoef, f0, vel_max):
     n = p.ndim * (8 * p.halo + 4)
     coeffs = np.zeros(n)
+    if p.ndim == 1:
+        # solve1D's CPML block (acoustic_1D.jl:118-125), the x block of 2D
+        q = Problem.from_buffer_copy(p)
+        q.ndim, q.ny, q.dy, q.freetop = 2, 3, p.dx, 0
+        c2 = np.zeros(2 * (8 * p.halo + 4))
+        lib().oracle_problem_coeffs(ctypes.byref(q), rcoef, f0, vel_max, _dp(c2))
+        coeffs[:] = c2[:n]
+        return coeffs
     lib().oracle_problem_coeffs(ctypes.byref(p), rcoef, f0, vel_max, _dp(coeffs))
     return coeffs
 
@@ -216,3 +226,60 @@ def max_threads():
 
 def last_loop_seconds():
     return lib().oracle_last_loop_seconds()
+
+
+def forward_1d(s):
+    """FP64 numpy restatement of the reference's 1D solver on a setup() dict
+    of a 1D problem (src/shared/acoustic_1D.jl): per step update_ψ! (:7-19,
+    both CPML ends, ψ on the half grid), update_p! (:21-48, ξ and the damping
+    term in the bands, i <= halo+1 and i >= nx-halo in 1-based indices),
+    inject_sources! (:50-56), record_receivers! (:58-64) and the
+    (pold, pcur, pnew) <- (pcur, pnew, pold) rotation of forward! (:66-88).
+    Returns (pfinal, traces)."""
+    p = s["problem"]
+    nx, h, nt = p.nx, p.halo, p.nt
+    dx = p.dx
+    _dx, _dx2 = 1.0 / dx, 1.0 / (dx * dx)
+    c = s["coeffs"]
+    a_l, a_r, bK_l, bK_r = c[0:h], c[h:2 * h], c[2 * h:3 * h], c[3 * h:4 * h]
+    hb = c[4 * h:]
+    a_hl, a_hr = hb[0:h + 1], hb[h + 1:2 * (h + 1)]
+    bK_hl, bK_hr = hb[2 * (h + 1):3 * (h + 1)], hb[3 * (h + 1):4 * (h + 1)]
+    fact = (p.dt * p.dt) * np.asarray(s["vel"], dtype=np.float64) ** 2
+    pold, pcur, pnew = np.zeros(nx), np.zeros(nx), np.zeros(nx)
+    psi_l, psi_r = np.zeros(h + 1), np.zeros(h + 1)
+    xi_l, xi_r = np.zeros(h), np.zeros(h)
+    src = np.asarray(s["possrcs"])[:, 0] - 1
+    rec = np.asarray(s["posrecs"])[:, 0] - 1
+    stf = s["dt2srctf"]
+    traces = np.zeros((nt, p.nrec), order="F")
+    i_in = np.arange(1, nx - 1)  # 0-based interior nodes
+    for it in range(nt):
+        # update_ψ!: entries i = 1..halo+1 (1-based), right side shifted
+        if h > 0:
+            q = np.arange(h + 1)
+            ii = q + nx - h - 2
+            psi_l = bK_hl * psi_l + a_hl * (pcur[q + 1] - pcur[q]) * _dx
+            psi_r = bK_hr * psi_r + a_hr * (pcur[ii + 1] - pcur[ii]) * _dx
+        # update_p!
+        d2p = (pcur[i_in + 1] - 2.0 * pcur[i_in] + pcur[i_in - 1]) * _dx2  # d2p[i0 - 1]
+        damp = np.zeros(nx - 2)
+        if h > 0:
+            # left band: 1-based i = 2 .. halo+1 (ψ entries i, i-1; ξ entry i-1)
+            il = np.arange(2, min(h + 1, nx - 1) + 1)
+            dpsi = (psi_l[il - 1] - psi_l[il - 2]) * _dx
+            xi_l[il - 2] = bK_l[il - 2] * xi_l[il - 2] + a_l[il - 2] * (d2p[il - 2] + dpsi)
+            damp[il - 2] = fact[il - 1] * (dpsi + xi_l[il - 2])
+            # right band: nx-halo <= i <= nx-1, not already in the left band
+            ir = np.arange(max(nx - h, h + 2), nx)
+            ii = ir - (nx - h) + 2
+            dpsi = (psi_r[ii - 1] - psi_r[ii - 2]) * _dx
+            xi_r[ii - 2] = bK_r[ii - 2] * xi_r[ii - 2] + a_r[ii - 2] * (d2p[ir - 2] + dpsi)
+            damp[ir - 2] = fact[ir - 1] * (dpsi + xi_r[ii - 2])
+        pnew[i_in] = 2.0 * pcur[i_in] - pold[i_in] + fact[i_in] * d2p + damp
+        for k, node in enumerate(src):
+            pnew[node] += stf[it, k]
+        for r, node in enumerate(rec):
+            traces[it, r] = pnew[node]
+        pold, pcur, pnew = pcur, pnew, pold
+    return pcur.copy(), traces

@@ -306,3 +306,78 @@ def test_config2_first_steps_vs_oracle(pkg, oracle, ctx, precision, tol):
     print(f"config2 nt=100 {precision}: traces {e_t:.3e} field {e_p:.3e}")
     assert np.abs(traces_o).max() > 0
     assert e_p <= tol and e_t <= tol
+
+
+# ---- 1D (the reference's solve1D) ------------------------------------------
+
+CASES1D = {
+    "analytic_halo0": lambda: __import__("test_oracle").analytic_case_1d(0),
+    "analytic_halo20": lambda: __import__("test_oracle").analytic_case_1d(20),
+    # heterogeneous line, two sources (one on the Dirichlet end), receivers in
+    # both bands and on a source node
+    "layered": lambda: ((3990.0,), 1.5, np.where(np.arange(400) < 250, 1800.0, 2600.0),
+                        [[1200.0], [0.0]], [0.08, 0.1], 12.0,
+                        [[100.0], [3900.0], [1200.0], [2600.0]],
+                        dict(halo=15, rcoef=1e-3, freetop=False)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES1D))
+@pytest.mark.parametrize("precision,tol", [("f64", TOL64), ("f32", TOL32)])
+def test_1d_vs_oracle(pkg, oracle, ctx, name, precision, tol):
+    lengths, lt, vel, sp, t0s, f0, rp, kw = CASES1D[name]()
+    srcs = pkg.Sources(sp, t0s, [pkg.rickersource1D] * len(t0s), f0)
+    recs = pkg.Receivers(rp)
+    s = pkg.prepare(lengths, lt, vel, srcs, recs, precision=precision, **kw)
+    p = s["problem"]
+    assert p.ndim == 1
+    traces = np.zeros((p.nt, p.nrec), order="F")
+    pend = np.zeros(vel.shape, order="F")
+    ctx.forward(p, s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"], s["posrecs"], traces, pend)
+    so = oracle.setup(lengths, lt, vel, sp, t0s, f0, rp, **kw)
+    pend_o, traces_o = oracle.forward_1d(so)
+    e_t, e_p = cases.rel_l2(traces, traces_o), cases.rel_l2(pend, pend_o)
+    print(f"1D {name} {precision}: traces rel-L2 {e_t:.3e}, field {e_p:.3e}")
+    assert np.abs(traces_o).max() > 0
+    assert e_t <= tol
+    if precision == "f64":
+        assert e_p <= tol
+
+
+def test_solve1D_api_analytic(pkg):
+    """test/test1D.jl:7-99 through solve1D (FP64 and FP32), halo 0 and 20."""
+    import test_oracle as T
+    from acousticwavecpml_b200.Acoustic1D import solve1D
+    for halo in (0, 20):
+        for precision in ("f64", "f32"):
+            lengths, lt, vel, sp, t0s, f0, rp, kw = T.analytic_case_1d(halo)
+            srcs = pkg.Sources(sp, t0s, [pkg.rickersource1D], f0)
+            recs = pkg.Receivers(rp)
+            kw.pop("freetop")
+            pend = solve1D(lengths[0], lt, vel, srcs, recs, precision=precision, verbose=False,
+                           **kw)
+            assert pend.shape == vel.shape
+            s = pkg.prepare(lengths, lt, vel, srcs, recs, **kw)
+            times, Gc = T.analytic_trace_1d(s["dt"], s["nt"], abs(sp[0][0] - rp[0][0]), 1.0,
+                                            t0s[0], f0)
+            err = T._trapz(times[1:], np.abs(recs.seismograms[:, 0] - Gc))
+            assert err <= np.max(np.abs(Gc)) * 0.01 * lt, (halo, precision, err)
+
+
+def test_1d_plan_snapshots_and_field(pkg, ctx):
+    lengths, lt, vel, sp, t0s, f0, rp, kw = CASES1D["layered"]()
+    srcs = pkg.Sources(sp, t0s, [pkg.rickersource1D] * len(t0s), f0)
+    s = pkg.prepare(lengths, lt, vel, srcs, pkg.Receivers(rp), precision="f64", **kw)
+    plan = ctx.plan(s["problem"], s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"],
+                    s["posrecs"])
+    ref = ctx.plan(s["problem"], s["vel"], s["coeffs"], s["possrcs"], s["dt2srctf"],
+                   s["posrecs"])
+    try:
+        snaps = plan.run_snapshots(100, 25)
+        for k in range(4):
+            ref.run(25)
+            np.testing.assert_array_equal(snaps[k], ref.field())
+            assert snaps[k].shape == vel.shape
+    finally:
+        plan.close()
+        ref.close()

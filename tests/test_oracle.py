@@ -165,3 +165,48 @@ def test_oracle_analytic_3d(oracle, halo):
     case = analytic_case_3d(halo)
     s, (_, traces) = _run(oracle, case)
     check_analytic(traces[:, 0], s, case, 3)
+
+
+# ---- 1D (src/shared/acoustic_1D.jl, test/test1D.jl) --------------------------
+
+def analytic_case_1d(halo):
+    """test/test1D.jl:7-52 (halo 0, lt = 10) and :54-99 (halo 20, lt = 20):
+    1001 nodes on 10 m, c0 = 1, Ricker f0 = 1 Hz, t0 = 4 s, source at lx/2,
+    receiver at lx/4."""
+    nx, lx = 1001, 10.0
+    return ((lx,), 10.0 if halo == 0 else 20.0, np.ones(nx), [[lx / 2]], [4.0], 1.0,
+            [[lx / 4]], dict(halo=halo, rcoef=1e-4, freetop=False))
+
+
+def analytic_trace_1d(dt, nt, dist, c0, t0, f0):
+    """test/test1D.jl:30-47: Heaviside Green's function 1/(2 c0) after the
+    arrival, convolved with the source times dt."""
+    times = np.arange(nt + 1) * dt
+    G = np.where(times - dist / c0 >= 0, 1.0 / (2 * c0), 0.0)
+    src = _ricker(times, t0, f0)
+    Gc = np.convolve(G, src * dt)[1:nt + 1]
+    return times, Gc
+
+
+@pytest.mark.parametrize("halo", [0, 20])
+def test_oracle_analytic_1d(oracle, halo):
+    lengths, lt, vel, sp, t0s, f0, rp, kw = analytic_case_1d(halo)
+    s = oracle.setup(lengths, lt, vel, sp, t0s, f0, rp, **kw)
+    assert s["dt"] == 10.0 / 1000 / 1.0 / 2
+    _, tr = oracle.forward_1d(s)
+    times, Gc = analytic_trace_1d(s["dt"], s["nt"], abs(sp[0][0] - rp[0][0]), 1.0, t0s[0], f0)
+    assert len(Gc) == s["nt"] == tr.shape[0]
+    err = _trapz(times[1:], np.abs(tr[:, 0] - Gc))
+    assert err <= np.max(np.abs(Gc)) * 0.01 * lt, err
+
+
+def test_oracle_1d_cpml_absorbs(oracle):
+    """With the CPML the 1D pulse leaves the line: after both arrivals the
+    field is far below its peak (without a band it stays reflected)."""
+    lengths, lt, vel, sp, t0s, f0, rp, kw = analytic_case_1d(20)
+    s = oracle.setup(lengths, 30.0, vel, sp, t0s, f0, rp, **kw)
+    pend, tr = oracle.forward_1d(s)
+    s0 = oracle.setup(lengths, 30.0, vel, sp, t0s, f0, rp, **dict(kw, halo=0))
+    pend0, _ = oracle.forward_1d(s0)
+    assert np.abs(pend).max() < 1e-2 * np.abs(tr).max()
+    assert np.abs(pend0).max() > 0.1 * np.abs(tr).max()
