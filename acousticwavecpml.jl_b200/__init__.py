@@ -13,7 +13,7 @@ The directory name is not a Python identifier; load it with
 """
 from . import Acoustic1D, Acoustic2D_CUDA, Acoustic3D_CUDA, adjoint  # noqa: F401
 from ._lib import AWC_F32, AWC_F64, AwcError, AwcInvalidArgument, Problem  # noqa: F401
-from . import batch  # noqa: F401
+from . import batch, models  # noqa: F401
 from .batch import (Batch, forward_batch, prepare_batch, solve2D_batch,  # noqa: F401
                     solve2D_batch_sharded, solve_sharded)
 from .core import Context, Plan, default_context, prepare  # noqa: F401
@@ -23,4 +23,4 @@ __all__ = ["Acoustic1D", "Acoustic2D_CUDA", "Acoustic3D_CUDA", "Sources", "Recei
            "calc_Kab_CPML", "Context", "Plan", "prepare", "default_context", "Problem",
            "AwcError", "AwcInvalidArgument", "AWC_F32", "AWC_F64", "Batch",
            "forward_batch", "prepare_batch", "adjoint", "solve2D_batch", "solve2D_batch_sharded",
-           "solve_sharded", "batch"]
+           "solve_sharded", "batch", "models"]

@@ -271,13 +271,21 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak, keep=None):
     ty, bps = b.get_launch()
     if keep is not None:  # traces of the first shot of each model (for the oracle check)
         first = {}
-        for k, sh in enumerate(w["shots"]):
-            first.setdefault(sh["model"], k)
-        for m, k in first.items():
-            if k % world == rank:
-                keep[k] = (w, b.traces(k // world))
+        for g, sh in enumerate(w["shots"]):
+            first.setdefault(sh["model"], g)
+        for g in first.values():
+            if g % world == rank:
+                keep[g] = (w, b.traces(g // world))
     b.close()
     achieved = words * 4 / t_ts / 1e9
+    traffic = ncu_traffic("step2d_batch_tma_96shots") if world == 1 else None
+    dram = None
+    if traffic:
+        dram = {"traffic_bytes_per_step": traffic, "achieved": traffic / t_ts / 1e9,
+                "frac": traffic / t_ts / 1e9 / peak,
+                "note": "real DRAM bytes (ncu, profiles/) per step over the measured step time: "
+                        "the 16 shots of a model share fact and the small models' fields "
+                        "partly stay in the 126 MB L2, so A_eff over-counts DRAM traffic"}
     return {"workload": w["name"], "shots": len(shots), "models": len(w["models"]),
             "nt": nt, "dtype": "f32", "value": len(shots) / (ms / 1e3 / k), "unit": "shots/s",
             "us_per_timestep": t_ts * 1e6, "gnodes_per_s": world * nodes / t_ts / 1e9,
@@ -287,6 +295,7 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak, keep=None):
                          "per_launch": "one time step of every shot of the rank's batch = one "
                                        "persistent batched-step launch; A_eff summed over "
                                        "shots, FP32 words"},
+            "dram_roofline": dram,
             "launch": {"tile": [64 if ty <= 16 else 32, ty], "blocks_per_sm": bps,
                        "kernel": "step2d_batch_tma (TMA stages, producer warp)" if ty <= 16
                                  else "step2d_batch (register strips)"},
@@ -513,9 +522,13 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src,
-                     "per_launch": "one time step = one fused step-kernel launch (sources "
-                                   "and receivers included); CUDA-event time of the graph "
-                                   "replays / launches"},
+                     "per_launch": "one time step: at depth 1 two kernel launches over "
+                                   "disjoint nodes (the band-free core box and the CPML "
+                                   "band boxes, parallel graph branches, sources and "
+                                   "receivers fused), at depth 2 half of one two-step pass; "
+                                   "achieved = A_eff of one step / CUDA-event time per step "
+                                   "of the graph replays; traffic = ncu DRAM bytes of one "
+                                   "step (both kernels)"},
         "gpu_launches": launches,
         "clocks": clocks,
     }
@@ -610,6 +623,10 @@ def main():
                           "restatement of the reference Threads path (Julia absent)",
                 "gcells_per_s": interior_cells(so["problem"]) / t_cpu / 1e9,
                 "s_per_timestep": t_cpu}
+            if "fp64" in line:
+                # like for like: the FP64 build against the FP64 CPU port, per cell update
+                line["fp64"]["vs_cpu_baseline_gcells"] = (line["fp64"]["gcells_per_s"] /
+                                                          line["cpu_baseline"]["gcells_per_s"])
 
     ctx.close()
     if rank == 0:

@@ -310,9 +310,16 @@ def test_config2_first_steps_vs_oracle(pkg, oracle, ctx, precision, tol):
 
 # ---- 1D (the reference's solve1D) ------------------------------------------
 
+def _analytic_1d_short(halo):
+    """test/test1D.jl's line, run for 8 s: the pulses are still on the line,
+    so the final field is not a residual far below the peak."""
+    case = __import__("test_oracle").analytic_case_1d(halo)
+    return case[:1] + (8.0,) + case[2:]
+
+
 CASES1D = {
-    "analytic_halo0": lambda: __import__("test_oracle").analytic_case_1d(0),
-    "analytic_halo20": lambda: __import__("test_oracle").analytic_case_1d(20),
+    "analytic_halo0": lambda: _analytic_1d_short(0),
+    "analytic_halo20": lambda: _analytic_1d_short(20),
     # heterogeneous line, two sources (one on the Dirichlet end), receivers in
     # both bands and on a source node
     "layered": lambda: ((3990.0,), 1.5, np.where(np.arange(400) < 250, 1800.0, 2600.0),
