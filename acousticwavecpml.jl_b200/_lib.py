@@ -115,6 +115,8 @@ SIGNATURES = {
                                              ctypes.POINTER(ctypes.c_int32),
                                              ctypes.POINTER(ctypes.c_int32)]),
     "awc_plan_launch_count": (ctypes.c_int64, [_vp, ctypes.c_int64]),
+    "awc_forward_decomposed": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int32, _PP, _vp, _vp,
+                                              _vp, _vp, _vp, _vp, _vp]),
     "awc_plan_run_snapshots": (ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int64, _vp,
                                               ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "awc_plan_set_wait": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),

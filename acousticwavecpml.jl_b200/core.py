@@ -84,6 +84,18 @@ _DEFAULT = {}
 _LOCK = threading.Lock()
 
 
+def forward_decomposed(contexts, problem, vel, coeffs, possrcs, dt2srctf, posrecs, traces,
+                       pfinal=None):
+    """awc_forward_decomposed: the shot split along its last axis into
+    len(contexts) subdomains, subdomain s on contexts[s] (the same context
+    may repeat), with a one-plane halo exchange per step."""
+    hs = (ctypes.c_void_p * len(contexts))(*[c.handle.value for c in contexts])
+    rc = _lib.lib().awc_forward_decomposed(hs, len(contexts), ctypes.byref(problem), _ptr(vel),
+                                           _ptr(coeffs), _ptr(possrcs), _ptr(dt2srctf),
+                                           _ptr(posrecs), _ptr(traces), _ptr(pfinal))
+    check(rc, contexts[0].handle)
+
+
 def default_context(device=0):
     """Per-device context shared by solve2D/solve3D calls of this process."""
     with _LOCK:

@@ -316,21 +316,60 @@ namespace {
     }                                                                             \
   } while (0)
 
-// Device memory of one adjoint run, freed on scope exit.
+// Device working memory of the adjoint, kept by the context between calls:
+// a run asks for its blocks in a fixed order, and a later run of the same
+// shape gets the same blocks back (no cudaMalloc/cudaFree, whose multi-GB
+// checkpoint arena otherwise costs more than the run). A block of another
+// size frees it and every later block. Contents are not kept: every run
+// initialises what it reads.
 struct DevMem {
-  std::vector<void*> ptrs;
-  ~DevMem() {
-    for (void* p : ptrs) cudaFree(p);
+  std::vector<std::pair<void*, size_t>> blocks;
+  size_t next = 0;
+  void begin() { next = 0; }
+  void release() {
+    for (auto& b : blocks) cudaFree(b.first);
+    blocks.clear();
+    next = 0;
   }
+  ~DevMem() { release(); }
   template <typename P>
   cudaError_t get(P** out, size_t bytes) {
+    bytes = std::max<size_t>(bytes, 16);
+    if (next < blocks.size()) {
+      if (blocks[next].second == bytes) {
+        *out = (P*)blocks[next++].first;
+        return cudaSuccess;
+      }
+      for (size_t k = next; k < blocks.size(); ++k) cudaFree(blocks[k].first);
+      blocks.resize(next);
+    }
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes, 16));
-    if (e == cudaSuccess) ptrs.push_back(p);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+      *out = nullptr;
+      return e;
+    }
+    blocks.emplace_back(p, bytes);
+    ++next;
     *out = (P*)p;
-    return e;
+    return cudaSuccess;
   }
 };
+
+// The context's adjoint memory (created on first use).
+DevMem& ctx_mem(awc_ctx* C) {
+  if (!C->adj_mem) {
+    DevMem* m = new DevMem();
+    C->adj_mem = m;
+    C->adj_release = [C]() {
+      delete static_cast<DevMem*>(C->adj_mem);
+      C->adj_mem = nullptr;
+    };
+  }
+  DevMem& m = *static_cast<DevMem*>(C->adj_mem);
+  m.begin();
+  return m;
+}
 
 // Interior node groups: each unique interior node of `pos` with its ids.
 struct Groups {
@@ -381,7 +420,7 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
   const int64_t nt = p->nt, nsrc = p->nsrc, nrec = p->nrec, h = p->halo;
   const int64_t NP = V.NP, fb = NP * (int64_t)sizeof(T);
   const bool want_grad = grad_out != nullptr;
-  DevMem mem;
+  DevMem& mem = ctx_mem(C);
   // adjoint fields
   T *lam[2], *G[2], *mu[3][2] = {}, *nu[3][2][2] = {};
   for (int b = 0; b < 2; ++b) {
@@ -655,14 +694,14 @@ int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
   if (!observed || !grad_c2 || !misfit)
     return awc::fail(ctx, AWC_ERR_INVALID, "observed/grad_c2/misfit is NULL");
   if (checkpoint_every < 1) return awc::fail(ctx, AWC_ERR_INVALID, "checkpoint_every must be >= 1");
-  awc_plan* plan = nullptr;
-  if ((rc = awc_plan_create(ctx, p, vel, coeffs, possrcs, dt2srctf, posrecs, &plan))) return rc;
+  if ((rc = awc::plan_for(ctx, &ctx->adj_plan, p, vel, coeffs, possrcs, dt2srctf, posrecs)))
+    return rc;
+  awc_plan* plan = ctx->adj_plan;
   rc = p->precision == AWC_F64
            ? adjoint_impl<double>(ctx, plan, p, possrcs, dt2srctf, posrecs, nullptr, observed,
                                   misfit, traces, checkpoint_every, grad_c2, nullptr)
            : adjoint_impl<float>(ctx, plan, p, possrcs, dt2srctf, posrecs, nullptr, observed,
                                  misfit, traces, checkpoint_every, grad_c2, nullptr);
-  awc_plan_destroy(plan);
   return rc;
 }
 
@@ -674,17 +713,17 @@ int awc_adjoint_sources(awc_ctx* ctx, const awc_problem* p, const double* vel,
   if ((rc = check_adjoint_problem(ctx, p))) return rc;
   if (!adjoint_traces || !src_out)
     return awc::fail(ctx, AWC_ERR_INVALID, "adjoint_traces/src_out is NULL");
-  awc_plan* plan = nullptr;
   // the plan only provides fact and the coefficients; the injected values
   // play no part in the transpose
   std::vector<double> zero(std::max<int64_t>(p->nt * p->nsrc, 1), 0.0);
-  if ((rc = awc_plan_create(ctx, p, vel, coeffs, possrcs, zero.data(), posrecs, &plan))) return rc;
+  if ((rc = awc::plan_for(ctx, &ctx->adj_plan, p, vel, coeffs, possrcs, zero.data(), posrecs)))
+    return rc;
+  awc_plan* plan = ctx->adj_plan;
   rc = p->precision == AWC_F64
            ? adjoint_impl<double>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces,
                                   nullptr, nullptr, nullptr, 1, nullptr, src_out)
            : adjoint_impl<float>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces,
                                  nullptr, nullptr, nullptr, 1, nullptr, src_out);
-  awc_plan_destroy(plan);
   return rc;
 }
 

@@ -1429,6 +1429,32 @@ PlanView plan_view(awc_plan* P) {
   return V;
 }
 
+int plan_for(awc_ctx* C, awc_plan** slot, const awc_problem* p, const double* vel,
+             const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
+             const int64_t* posrecs) {
+  awc_plan* P = *slot;
+  if (P && p && p->ndim != 1 && !P->is1d && same_shape(P->p, *p)) {
+    int rc;
+    if ((rc = validate(p, &C->err)) ||
+        (rc = check_positions(p, possrcs, p->nsrc, "source", &C->err)) ||
+        (rc = check_positions(p, posrecs, p->nrec, "receiver", &C->err)))
+      return rc;
+    if (!vel || !coeffs || (p->nsrc > 0 && p->nt > 0 && !dt2srctf))
+      return set_err(&C->err, AWC_ERR_INVALID, "vel/coeffs/dt2srctf is NULL");
+    CUDA_TRY(&C->err, cudaSetDevice(C->device));
+    P->p = *p;
+    if (p->ndim == 2) P->p.nz = 1;
+    P->depth = 1;
+    if ((rc = plan_upload(P, vel, coeffs, possrcs, dt2srctf, posrecs))) return rc;
+    return awc_plan_reset(P);
+  }
+  if (P) {
+    awc_plan_destroy(P);
+    *slot = nullptr;
+  }
+  return awc_plan_create(C, p, vel, coeffs, possrcs, dt2srctf, posrecs, slot);
+}
+
 void plan_set_step(awc_plan* P, int64_t step) {
   P->step = step;
   P->state = StepState::after_steps(step);
@@ -1536,6 +1562,10 @@ void awc_destroy(awc_ctx* ctx) {
   cudaSetDevice(ctx->device);
   for (awc_plan* P : ctx->cache) delete P;
   ctx->cache.clear();
+  if (ctx->adj_release) ctx->adj_release();
+  ctx->adj_release = nullptr;
+  if (ctx->adj_plan) delete ctx->adj_plan;
+  ctx->adj_plan = nullptr;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->stream2) cudaStreamSynchronize(ctx->stream2);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -2021,6 +2051,227 @@ int awc_forward(awc_ctx* ctx, const awc_problem* p, const double* vel, const dou
   if ((rc = awc_plan_run(P, p->nt, 1, &ctx->last_run_ms))) return rc;
   if (traces && (rc = awc_plan_traces(P, traces))) return rc;
   if (pfinal && (rc = awc_plan_field(P, pfinal))) return rc;
+  return AWC_OK;
+}
+
+int awc_forward_decomposed(awc_ctx* const* ctxs, int32_t nsub, const awc_problem* p,
+                           const double* vel, const double* coeffs, const int64_t* possrcs,
+                           const double* dt2srctf, const int64_t* posrecs, double* traces,
+                           double* pfinal) {
+  std::string terr;
+  if (!ctxs || nsub < 1) return set_err(nullptr, AWC_ERR_INVALID, "ctxs is NULL or nsub < 1");
+  for (int32_t s = 0; s < nsub; ++s)
+    if (!ctxs[s]) return set_err(nullptr, AWC_ERR_INVALID, "ctxs[%d] is NULL", s);
+  awc_ctx* C0 = ctxs[0];
+  int rc;
+  if ((rc = validate(p, &C0->err))) return rc;
+  if (!vel || !coeffs) return set_err(&C0->err, AWC_ERR_INVALID, "vel/coeffs are NULL");
+  if (p->nsrc > 0 && p->nt > 0 && !dt2srctf)
+    return set_err(&C0->err, AWC_ERR_INVALID, "dt2srctf is NULL");
+  if ((rc = check_positions(p, possrcs, p->nsrc, "source", &C0->err)) ||
+      (rc = check_positions(p, posrecs, p->nrec, "receiver", &C0->err)))
+    return rc;
+  if (p->nt * p->nrec > 0 && !traces) return set_err(&C0->err, AWC_ERR_INVALID, "traces is NULL");
+  const int ax = p->ndim - 1;  // the split axis: y in 2D, z in 3D
+  const int64_t nx = p->nx, ny = p->ny, nz = p->ndim == 3 ? p->nz : 1;
+  const int64_t n = ax == 2 ? nz : ny, ni = n - 2, h = p->halo;
+  // contiguous interior ranges [a_s, b_s] (global, 0-based) of nearly equal size
+  std::vector<int64_t> a(nsub), b(nsub);
+  for (int32_t s = 0; s < nsub; ++s) {
+    a[s] = 1 + ni * s / nsub;
+    b[s] = ni * (s + 1) / nsub;
+    if (b[s] < a[s])
+      return set_err(&C0->err, AWC_ERR_INVALID, "%d subdomains for %lld interior planes",
+                     nsub, (long long)ni);
+  }
+  // the outer subdomains hold the whole CPML band of the split axis
+  if (nsub > 1 && h > 0 && (b[0] - a[0] + 3 < 2 * h + 2 || b[nsub - 1] - a[nsub - 1] + 3 < 2 * h + 2))
+    return set_err(&C0->err, AWC_ERR_INVALID,
+                   "the first and last subdomains need at least 2 halo + 2 planes along the "
+                   "split axis (use fewer subdomains)");
+  const int64_t clen = awc_coeffs_len(p), blk = 8 * h + 4;
+  auto plane_of = [&](const int64_t* pos, int64_t cnt, int64_t r) { return pos[r + cnt * ax] - 1; };
+  auto owner = [&](int64_t g) -> int32_t {  // subdomain holding global plane g
+    if (g <= a[0]) return 0;
+    for (int32_t s = 0; s < nsub; ++s)
+      if (g >= a[s] && g <= b[s]) return s;
+    return nsub - 1;  // the far rim plane
+  };
+  struct Sub {
+    awc_problem p{};
+    std::vector<double> vel, coeffs, stf;
+    std::vector<int64_t> ps, pr, sid, rid;
+    awc_plan* plan = nullptr;
+    cudaEvent_t stepped = nullptr, filled = nullptr;
+  };
+  std::vector<Sub> sub(nsub);
+  auto cleanup = [&]() {
+    for (Sub& u : sub) {
+      if (u.plan) awc_plan_destroy(u.plan);
+      if (u.stepped) cudaEventDestroy(u.stepped);
+      if (u.filled) cudaEventDestroy(u.filled);
+    }
+  };
+  for (int32_t s = 0; s < nsub; ++s) {
+    Sub& u = sub[s];
+    const int64_t g0 = a[s] - 1, nl = b[s] - a[s] + 3;  // local plane l = global g0 + l
+    u.p = *p;
+    (ax == 2 ? u.p.nz : u.p.ny) = nl;
+    u.p.freetop = ax == 1 && s > 0 ? 0 : p->freetop;
+    // velocity slab
+    const int64_t per = ax == 2 ? nx * ny : nx;          // values per plane
+    const int64_t rows = ax == 2 ? 1 : 1, outer = ax == 2 ? 1 : nz;  // 2D: one "outer" block
+    (void)rows;
+    u.vel.resize((size_t)(per * nl * outer));
+    for (int64_t o = 0; o < outer; ++o)
+      for (int64_t l = 0; l < nl; ++l)
+        std::memcpy(&u.vel[(size_t)((o * nl + l) * per)], vel + (o * n + g0 + l) * per,
+                    per * sizeof(double));
+    // CPML coefficients: the split axis keeps only the outer sides' bands
+    u.coeffs.assign(coeffs, coeffs + clen);
+    double* zb = u.coeffs.data() + ax * blk;
+    for (int side = 0; side < 2; ++side) {
+      const bool inner = side == 0 ? s > 0 : s < nsub - 1;
+      if (!inner) continue;
+      for (int64_t m = 0; m < h; ++m) {
+        zb[side * h + m] = 0.0;
+        zb[2 * h + side * h + m] = 1.0;
+      }
+      for (int64_t m = 0; m < h + 1; ++m) {
+        zb[4 * h + side * (h + 1) + m] = 0.0;
+        zb[4 * h + 2 * (h + 1) + side * (h + 1) + m] = 1.0;
+      }
+    }
+    // the sources and receivers this subdomain owns, in local coordinates
+    auto take = [&](const int64_t* pos, int64_t cnt, std::vector<int64_t>& out,
+                    std::vector<int64_t>& ids) {
+      ids.clear();
+      for (int64_t r = 0; r < cnt; ++r)
+        if (owner(plane_of(pos, cnt, r)) == s) ids.push_back(r);
+      const int64_t m = (int64_t)ids.size();
+      out.assign((size_t)std::max<int64_t>(m * p->ndim, 1), 1);
+      for (int64_t e = 0; e < m; ++e)
+        for (int d = 0; d < p->ndim; ++d)
+          out[e + m * d] = pos[ids[e] + cnt * d] - (d == ax ? g0 : 0);
+    };
+    take(possrcs, p->nsrc, u.ps, u.sid);
+    take(posrecs, p->nrec, u.pr, u.rid);
+    u.p.nsrc = (int64_t)u.sid.size();
+    u.p.nrec = (int64_t)u.rid.size();
+    u.stf.assign((size_t)std::max<int64_t>(p->nt * u.p.nsrc, 1), 0.0);
+    for (size_t e = 0; e < u.sid.size(); ++e)
+      std::memcpy(&u.stf[e * p->nt], dt2srctf + u.sid[e] * p->nt, p->nt * sizeof(double));
+    if ((rc = awc_plan_create(ctxs[s], &u.p, u.vel.data(), u.coeffs.data(), u.ps.data(),
+                              u.stf.data(), u.pr.data(), &u.plan))) {
+      cleanup();
+      return rc;
+    }
+    awc_ctx* C = ctxs[s];
+    if (cudaSetDevice(C->device) != cudaSuccess ||
+        cudaEventCreateWithFlags(&u.stepped, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&u.filled, cudaEventDisableTiming) != cudaSuccess ||
+        (rc = prepare_launch(u.plan))) {
+      cleanup();
+      return rc ? rc : set_err(&C->err, AWC_ERR_CUDA, "event creation failed");
+    }
+  }
+  // time loop: every subdomain advances one step, then the planes next to
+  // each interface cross it (one-plane halo exchange, update_halo! of
+  // acoustic_3D_multixPU.jl:221): subdomain s's last interior plane becomes
+  // s+1's plane 0, s+1's first interior plane becomes s's last plane
+  auto plane_ptr = [&](Sub& u, int64_t l) {
+    awc_plan* P = u.plan;
+    const int64_t stride = ax == 2 ? P->px * ny : P->px;  // elements per plane
+    return (char*)P->buf[P->state.ord[0]] + l * stride * P->esz;
+  };
+  const size_t plane_bytes = (size_t)((ax == 2 ? sub[0].plan->px * ny : sub[0].plan->px) *
+                                      sub[0].plan->esz);
+  for (int64_t it = 0; it < p->nt; ++it) {
+    for (int32_t s = 0; s < nsub; ++s) {
+      Sub& u = sub[s];
+      awc_ctx* C = ctxs[s];
+      cudaSetDevice(C->device);
+      if (it > 0)  // the copies into and out of this subdomain's planes are done
+        for (int32_t t : {s - 1, s + 1})
+          if (t >= 0 && t < nsub && cudaStreamWaitEvent(C->stream, sub[t].filled, 0) != cudaSuccess) {
+            cleanup();
+            return set_err(&C->err, AWC_ERR_CUDA, "stream wait failed");
+          }
+      StepState stt = u.plan->state;
+      if ((rc = launch_range(u.plan, it, 1, stt, C->stream))) {
+        cleanup();
+        return rc;
+      }
+      u.plan->state = stt;
+      u.plan->step = it + 1;
+      cudaEventRecord(u.stepped, C->stream);
+    }
+    for (int32_t s = 0; s < nsub; ++s) {
+      Sub& u = sub[s];
+      awc_ctx* C = ctxs[s];
+      cudaSetDevice(C->device);
+      const int64_t nl = ax == 2 ? u.p.nz : u.p.ny;
+      cudaError_t e = cudaSuccess;
+      if (s > 0) {  // plane 0 <- the left neighbour's last interior plane
+        Sub& v = sub[s - 1];
+        const int64_t nv = ax == 2 ? v.p.nz : v.p.ny;
+        e = cudaStreamWaitEvent(C->stream, v.stepped, 0);
+        if (e == cudaSuccess)
+          e = cudaMemcpyPeerAsync(plane_ptr(u, 0), C->device, plane_ptr(v, nv - 2),
+                                  ctxs[s - 1]->device, plane_bytes, C->stream);
+      }
+      if (e == cudaSuccess && s + 1 < nsub) {  // last plane <- the right neighbour's plane 1
+        Sub& v = sub[s + 1];
+        e = cudaStreamWaitEvent(C->stream, v.stepped, 0);
+        if (e == cudaSuccess)
+          e = cudaMemcpyPeerAsync(plane_ptr(u, nl - 1), C->device, plane_ptr(v, 1),
+                                  ctxs[s + 1]->device, plane_bytes, C->stream);
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(u.filled, C->stream);
+      if (e != cudaSuccess) {
+        cleanup();
+        return set_err(&C->err, AWC_ERR_CUDA, "halo exchange failed: %s", cudaGetErrorString(e));
+      }
+    }
+  }
+  for (int32_t s = 0; s < nsub; ++s) {
+    cudaSetDevice(ctxs[s]->device);
+    if (cudaStreamSynchronize(ctxs[s]->stream) != cudaSuccess ||
+        (rc = check_device_flag(sub[s].plan))) {
+      cleanup();
+      return rc ? rc : set_err(&ctxs[s]->err, AWC_ERR_CUDA, "decomposed run failed");
+    }
+  }
+  // outputs: each subdomain's receivers, and its interior planes of the field
+  for (int32_t s = 0; s < nsub && p->nt * p->nrec > 0; ++s) {
+    Sub& u = sub[s];
+    if (u.p.nrec == 0) continue;
+    std::vector<double> tr((size_t)(p->nt * u.p.nrec));
+    if ((rc = awc_plan_traces(u.plan, tr.data()))) {
+      cleanup();
+      return rc;
+    }
+    for (size_t e = 0; e < u.rid.size(); ++e)
+      std::memcpy(traces + u.rid[e] * p->nt, &tr[e * p->nt], p->nt * sizeof(double));
+  }
+  if (pfinal) {
+    const int64_t per = ax == 2 ? nx * ny : nx, outer = ax == 2 ? 1 : nz;
+    for (int32_t s = 0; s < nsub; ++s) {
+      Sub& u = sub[s];
+      const int64_t nl = ax == 2 ? u.p.nz : u.p.ny, g0 = a[s] - 1;
+      std::vector<double> f((size_t)(per * nl * outer));
+      if ((rc = awc_plan_field(u.plan, f.data()))) {
+        cleanup();
+        return rc;
+      }
+      const int64_t l0 = s == 0 ? 0 : 1, l1 = s == nsub - 1 ? nl - 1 : nl - 2;
+      for (int64_t o = 0; o < outer; ++o)
+        for (int64_t l = l0; l <= l1; ++l)
+          std::memcpy(pfinal + (o * n + g0 + l) * per, &f[(size_t)((o * nl + l) * per)],
+                      per * sizeof(double));
+    }
+  }
+  cleanup();
   return AWC_OK;
 }
 

@@ -5,8 +5,11 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <functional>
 #include <string>
 #include <vector>
+
+#include "../../include/awcpml.h"
 
 struct awc_plan;
 
@@ -21,6 +24,11 @@ struct awc_ctx {
   float last_run_ms = 0.f;
   int64_t autotune_steps = 10;   // per candidate, for new 3D plans of awc_forward
   std::vector<awc_plan*> cache;  // plans reused by awc_forward, most recent last
+  // the adjoint entry points keep their plan and working memory between
+  // calls of one shape (released by awc_destroy or a call of another shape)
+  awc_plan* adj_plan = nullptr;
+  void* adj_mem = nullptr;
+  std::function<void()> adj_release;
 };
 
 namespace awc {
@@ -47,6 +55,12 @@ void plan_set_step(awc_plan* P, int64_t step);
 // During eager runs, copies the new field of each step it in [first,
 // first + count) to dst[it - first] (stream-ordered); NULL stops it.
 void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count);
+
+// Re-uploads a new shot into *slot when it holds a plan of the same shape
+// (same buffers), else replaces it by a new plan. The plan is reset.
+int plan_for(awc_ctx* C, awc_plan** slot, const awc_problem* p, const double* vel,
+             const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
+             const int64_t* posrecs);
 
 // Sets the calling thread's last error (awc_last_error(NULL)) and, when ctx
 // is not NULL, the context's; returns code.

@@ -125,6 +125,24 @@ int awc_forward(awc_ctx* ctx, const awc_problem* p, const double* vel, const dou
                 const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
                 double* traces, double* pfinal);
 
+/* Domain decomposition, the reference's multi-process strategy
+ * (solve2D_multi/solve3D_multi, src/shared/acoustic_3D_multixPU.jl:157-230:
+ * each rank updates its subdomain, then update_halo! exchanges one plane per
+ * interface): the problem of awc_forward split along its last axis (y in
+ * 2D, z in 3D) into nsub contiguous subdomains of nearly equal size, each a
+ * plan on ctxs[s] with a halo plane on each inner side. Every time step all
+ * subdomains advance, then each interface's two planes cross it (peer copies
+ * when the contexts sit on different devices; a context may appear several
+ * times, its subdomains then take turns on its stream). The CPML of the
+ * split axis stays on the outer subdomains, which need at least 2 halo + 2
+ * planes along it. Sources and receivers belong to the subdomain that
+ * updates their node. Results (traces, final field) are bitwise those of
+ * awc_forward. No sources or receivers are exchanged: only field planes. */
+int awc_forward_decomposed(awc_ctx* const* ctxs, int32_t nsub, const awc_problem* p,
+                           const double* vel, const double* coeffs, const int64_t* possrcs,
+                           const double* dt2srctf, const int64_t* posrecs, double* traces,
+                           double* pfinal);
+
 /* Device-resident plan: the inputs of awc_forward uploaded once, the state
  * kept in HBM between calls. awc_forward is plan create + run(nt) + read-out.
  * The plan belongs to its context and must be destroyed before it. */
@@ -256,8 +274,12 @@ int awc_forward_batch(awc_ctx* ctx, int32_t nmodels, const awc_problem* models,
  * No counterpart in the reference, which has no gradient. Both entry points
  * run the exact discrete transpose of the time step above (awc_forward's
  * arithmetic for fixed c), backwards in time, on the interior nodes. They
- * need CPML bands that do not overlap (n >= 2 halo + 2 on each axis) and
- * allocate their working memory for the duration of the call.
+ * need CPML bands that do not overlap (n >= 2 halo + 2 on each axis). Their
+ * plan and working memory (nt / checkpoint_every saved states, the
+ * checkpoint_every + 2 pressure fields of a segment and the adjoint fields)
+ * stay allocated in the context between calls of one shape, so that a
+ * sequence of gradients of one survey allocates once; a call of another
+ * shape replaces them and awc_destroy frees them.
  *
  * awc_misfit_gradient: J = 1/2 Σ_t Σ_r (traces[t,r] - observed[t,r])² of the
  * shot described like awc_forward, and dJ/d(c²) per node (nx*ny[*nz],
