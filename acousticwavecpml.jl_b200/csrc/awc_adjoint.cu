@@ -55,87 +55,244 @@
 
 namespace awc {
 
+// Parameters of one adjoint step t (the kernels compute λ_{t+1}). The band
+// state advances inside the same launch: a band node forms ν_{t+2} and
+// μ_{t+2} of its own entries and faces from ν_{t+3}, μ_{t+3} and
+// G_{t+2} = F λ_{t+2}, as the update formulas above give them, and, for its
+// λ_{t+1}, also those of its axis neighbours (the same pinned arithmetic, so
+// the values agree bitwise with what their owners store). G is formed where
+// it is used, from F and λ_{t+2}.
 template <typename T>
-struct AdjParams {
-  int32_t ndim, nx, ny, nz, halo;
+struct AdjStep {
+  int32_t nx, ny, nz, halo;
   int64_t px, plane;
   T inv_d[3], inv_d2[3];
   const T* F;
-  const T* G;     // F λ_{t+2} on the interior, 0 on the rim
-  const T* lam2;  // λ_{t+2}
-  const T* lam3;  // λ_{t+3}
-  T* lamn;        // λ_{t+1} (may alias lam3: read and written at the same node)
-  T* mu[3][2];    // μ, updated in place (layout of ψ)
-  const T* nu_old[3][2];  // ν_{t+2} (layout of ξ)
-  T* nu_new[3][2];        // ν_{t+1}
+  const T* lam2;   // λ_{t+2}
+  T* lam;          // in: λ_{t+3} less the residuals of step t; out: λ_{t+1}
+  const T* pm1;    // p_{t-1}, p_t, p_{t+1} (gradient mode)
+  const T* p0;
+  const T* pp1;
+  double* grad;    // dJ/dF accumulator (gradient mode)
+  const T* nu_in[3][2];  // ν_{t+3} (layout of ξ)
+  T* nu_out[3][2];       // ν_{t+2}
+  const T* mu_in[3][2];  // μ_{t+3} (layout of ψ)
+  T* mu_out[3][2];       // μ_{t+2}
   const T* a[3][2];
   const T* bK[3][2];
   const T* ah[3][2];
   const T* bKh[3][2];
   int32_t active[3][2];
-  int32_t off[3][2];  // band node c has entry q = c - off
+  int32_t off[3][2];     // band node c has entry q = c - off
+  // nodes farther than one node from every active band (the core kernel)
+  Box core;
+  // disjoint boxes covering the other interior nodes (the shell kernel); box
+  // b owns blocks [box_blk[b], box_blk[b+1]). Box.kind = zx + 3 zy + 9 zz
+  // names the band zone of its nodes per axis (0 none, 1 next to or in the
+  // left band, 2 the right one); kind ADJ_GENERIC boxes test every node.
+  int32_t nbox;
+  Box box[27];
+  int32_t box_blk[28];
 };
+constexpr int ADJ_GENERIC = 27;
 
-// Element index of entry e of a band array (ψ: h+1 layers, ξ: h layers) of
-// axis a at the node (i, j, k) (the node's own axis coordinate is replaced
-// by e): x (layers, ny, nz); y (px, layers, nz); z (px, ny, layers).
-template <typename T>
-__device__ __forceinline__ int64_t band_index(const AdjParams<T>& A, int a, int layers, int e,
-                                              int i, int j, int k) {
-  if (a == 0) return e + (int64_t)layers * (j + (int64_t)A.ny * k);
-  if (a == 1) return i + A.px * (e + (int64_t)layers * k);
-  return i + A.px * (j + (int64_t)A.ny * e);
+// Element index of entry 0 of the band array (`layers` entries along axis a)
+// at the node (i, j, k), and the step from one entry to the next: x
+// (layers, ny, nz); y (px, layers, nz); z (px, ny, layers).
+template <typename I, typename T>
+__device__ __forceinline__ I band_base(const AdjStep<T>& A, int a, int layers, int i, int j,
+                                       int k) {
+  if (a == 0) return (I)layers * ((I)j + (I)A.ny * (I)k);
+  if (a == 1) return (I)i + (I)A.px * (I)layers * (I)k;
+  return (I)i + (I)A.px * (I)j;
+}
+template <typename I, typename T>
+__device__ __forceinline__ I band_step(const AdjStep<T>& A, int a) {
+  return a == 0 ? (I)1 : a == 1 ? (I)A.px : (I)A.plane;
 }
 
-// a ν_{t+2} of axis a at the node whose axis coordinate is c (other
-// coordinates i, j, k), when it is a band node of that axis.
-template <typename T>
-__device__ __forceinline__ T adj_anu(const AdjParams<T>& A, int a, int c, int i, int j, int k) {
-  T g = 0;
-  for (int s = 0; s < 2; ++s) {
-    if (!A.active[a][s]) continue;
-    const int q = c - A.off[a][s];
-    if (q >= 1 && q <= A.halo)
-      g += A.a[a][s][q - 1] * A.nu_old[a][s][band_index(A, a, A.halo, q - 1, i, j, k)];
+// The band part of λ_{t+1} along axis a from side s at a node with entry
+// q in [0, h+1] (q = 0 and h+1 are the nodes next to the band), given
+// G_{t+2} at the nodes c-1, c, c+1 of the axis (m = 0, 1, 2; entries q-1,
+// q, q+1; ν index e = q-2+m):
+//   ν_{t+2}[e] = bK_e ν_{t+3}[e] + G,   w = a_e ν_{t+2}[e] + G,
+//   μ_{t+2}[f] = bKh_f μ_{t+3}[f] + (w_f - w_{f+1}) / d   (faces f = q-1, q),
+// result (a ν(c+1) - 2 a ν(c) + a ν(c-1)) / d² + (ah μ[q-1] - ah μ[q]) / d.
+// The node stores ν_{t+2}[q-1] and μ_{t+2}[q] when 1 <= q <= h, and
+// μ_{t+2}[0] when q = 1.
+template <typename T, typename I>
+__device__ __forceinline__ T adj_side(const AdjStep<T>& A, int a, int s, int q, int i, int j,
+                                      int k, T gm, T gc, T gp) {
+  const int h = A.halo;
+  const I step = band_step<I>(A, a);
+  const I nb = band_base<I>(A, a, h, i, j, k), mb = band_base<I>(A, a, h + 1, i, j, k);
+  const T* __restrict__ ca = A.a[a][s];
+  const T* __restrict__ cbK = A.bK[a][s];
+  const T* __restrict__ nu_in = A.nu_in[a][s];
+  const T gv[3] = {gm, gc, gp};
+  T w[3], anu[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const int e = q - 2 + m;
+    w[m] = T(0);
+    anu[m] = T(0);
+    if (e >= 0 && e < h) {
+      const T nu = fma(__ldg(cbK + e), __ldg(nu_in + nb + (I)e * step), gv[m]);
+      const T ae = __ldg(ca + e);
+      anu[m] = mul_rn(ae, nu);
+      w[m] = fma(ae, nu, gv[m]);
+      if (m == 1) A.nu_out[a][s][nb + (I)e * step] = nu;
+    }
   }
-  return g;
-}
-
-// Whether axis coordinate c lies within one node of a band (of any side).
-template <typename T>
-__device__ __forceinline__ bool adj_band_near(const AdjParams<T>& A, int c, int n) {
-  return A.halo > 0 && (c <= A.halo + 1 || c >= n - A.halo - 2);
-}
-
-// The band part of λ_{t+1} along axis a at node (i, j, k) whose axis
-// coordinate is c: the transposed stencil of a ν_{t+2} and the ψ-face terms,
-// non-zero only within one node of a band.
-template <typename T>
-__device__ __forceinline__ T adj_band_terms(const AdjParams<T>& A, int a, int c, int n, int i,
-                                            int j, int k) {
-  if (A.halo == 0 || (c > A.halo + 1 && c < n - A.halo - 2)) return T(0);
-  const int di = a == 0, dj = a == 1, dk = a == 2;
-  T acc = T(-2) * adj_anu(A, a, c, i, j, k);
-  if (c + 1 <= n - 2) acc += adj_anu(A, a, c + 1, i + di, j + dj, k + dk);
-  if (c - 1 >= 1) acc += adj_anu(A, a, c - 1, i - di, j - dj, k - dk);
-  T r = A.inv_d2[a] * acc;
-  for (int s = 0; s < 2; ++s) {
-    if (!A.active[a][s]) continue;
-    const int e1 = c - 1 - A.off[a][s], e2 = c - A.off[a][s];
-    T f = 0;
-    if (e1 >= 0 && e1 <= A.halo)
-      f += A.ah[a][s][e1] * A.mu[a][s][band_index(A, a, A.halo + 1, e1, i, j, k)];
-    if (e2 >= 0 && e2 <= A.halo)
-      f -= A.ah[a][s][e2] * A.mu[a][s][band_index(A, a, A.halo + 1, e2, i, j, k)];
-    r += A.inv_d[a] * f;
+  const T inv_d = A.inv_d[a];
+  const T* __restrict__ cbKh = A.bKh[a][s];
+  const T* __restrict__ cah = A.ah[a][s];
+  const T* __restrict__ mu_in = A.mu_in[a][s];
+  T* __restrict__ mu_out = A.mu_out[a][s];
+  T f = T(0);
+  if (q >= 1) {  // face q - 1
+    const int e = q - 1;
+    const T mu = fma(__ldg(cbKh + e), __ldg(mu_in + mb + (I)e * step), mul_rn(inv_d, w[0] - w[1]));
+    f = mul_rn(__ldg(cah + e), mu);
+    if (q == 1) mu_out[mb] = mu;
   }
-  return r;
+  if (q <= h) {  // face q
+    const T mu = fma(__ldg(cbKh + q), __ldg(mu_in + mb + (I)q * step), mul_rn(inv_d, w[1] - w[2]));
+    f = f - mul_rn(__ldg(cah + q), mu);
+    if (q >= 1) mu_out[mb + (I)q * step] = mu;
+  }
+  const T acc = (anu[2] - T(2) * anu[1]) + anu[0];
+  return fma(A.inv_d2[a], acc, mul_rn(inv_d, f));
 }
 
-// The residuals of step t enter λ_{t+1} = R_t + 2 λ_{t+2} - λ_{t+3} + ...
-// through λ_{t+3}: before adj_lambda_grad runs, λ_{t+3} -= R_t at the receiver
-// nodes (one thread per node, its receivers in receiver order), so that the
-// fused kernel needs no receiver lookup.
+// G_{t+2} = F λ_{t+2} at node o + d.
+template <typename T, typename I>
+__device__ __forceinline__ T adj_g(const AdjStep<T>& A, I o) {
+  return mul_rn(__ldg(A.F + o), __ldg(A.lam2 + o));
+}
+
+// The node update at o: λ_{t+1} = 2 λ_{t+2} - λ_{t+3} + the transposed
+// stencil lap of G_{t+2} + band, and the gradient accumulation
+// dJ/dF += λ_{t+1} B_t with B_t the Laplacian of p_t (in the working
+// precision) at nodes outside every active band, (p_{t+1} - 2 p_t + p_{t-1})
+// / F (in double) inside one, where adj_sources removes the source term.
+template <typename T, typename I, int ND, bool GRAD>
+__device__ __forceinline__ void adj_update(const AdjStep<T>& A, I o, T l2, T f, T lap, T band,
+                                           bool in_band) {
+  const T lam = (T(2) * l2 - A.lam[o]) + (lap + band);
+  if (GRAD) {
+    const T* __restrict__ P = A.p0;
+    const T c = __ldg(P + o);
+    double b;
+    if (in_band) {
+      b = (((double)__ldg(A.pp1 + o) - 2.0 * (double)c) + (double)__ldg(A.pm1 + o)) / (double)f;
+    } else {
+      const I px = (I)A.px;
+      T bl = second_diff(__ldg(P + o - 1), c, __ldg(P + o + 1), A.inv_d2[0]) +
+             second_diff(__ldg(P + o - px), c, __ldg(P + o + px), A.inv_d2[1]);
+      if (ND == 3) {
+        const I pl = (I)A.plane;
+        bl += second_diff(__ldg(P + o - pl), c, __ldg(P + o + pl), A.inv_d2[2]);
+      }
+      b = (double)bl;
+    }
+    A.grad[o] += (double)lam * b;
+  }
+  A.lam[o] = lam;
+}
+
+// Nodes of the core box: blocks of 32 x 8 (x, y) nodes of one z plane.
+template <typename T, typename I, int ND, bool GRAD>
+__global__ void __launch_bounds__(256) adj_core(const __grid_constant__ AdjStep<T> A) {
+  const int i = A.core.x0 + blockIdx.x * 32 + threadIdx.x;
+  const int j = A.core.y0 + blockIdx.y * 8 + threadIdx.y;
+  const int k = ND == 3 ? A.core.z0 + (int)blockIdx.z : 0;
+  if (i > A.core.x1 || j > A.core.y1) return;
+  const I px = (I)A.px, pl = (I)A.plane;
+  const I o = (I)i + px * (I)j + pl * (I)k;
+  const T f = __ldg(A.F + o), l2 = __ldg(A.lam2 + o);
+  const T gc = mul_rn(f, l2);
+  T lap = second_diff(adj_g(A, o - 1), gc, adj_g(A, o + 1), A.inv_d2[0]) +
+          second_diff(adj_g(A, o - px), gc, adj_g(A, o + px), A.inv_d2[1]);
+  if (ND == 3) lap += second_diff(adj_g(A, o - pl), gc, adj_g(A, o + pl), A.inv_d2[2]);
+  adj_update<T, I, ND, GRAD>(A, o, l2, f, lap, T(0), false);
+}
+
+// One shell node whose band zone per axis is ZX, ZY, ZZ (0 none, 1 left, 2
+// right; 3 unknown: both sides tested at run time).
+template <typename T, typename I, int ND, bool GRAD, int ZX, int ZY, int ZZ>
+__device__ __forceinline__ void adj_shell_node(const AdjStep<T>& A, int i, int j, int k) {
+  const I px = (I)A.px, pl = (I)A.plane;
+  const I o = (I)i + px * (I)j + pl * (I)k;
+  const T f = __ldg(A.F + o), l2 = __ldg(A.lam2 + o);
+  const T gc = mul_rn(f, l2);
+  const T g[3][2] = {{adj_g(A, o - 1), adj_g(A, o + 1)},
+                     {adj_g(A, o - px), adj_g(A, o + px)},
+                     {ND == 3 ? adj_g(A, o - pl) : T(0), ND == 3 ? adj_g(A, o + pl) : T(0)}};
+  T lap = second_diff(g[0][0], gc, g[0][1], A.inv_d2[0]) +
+          second_diff(g[1][0], gc, g[1][1], A.inv_d2[1]);
+  if (ND == 3) lap += second_diff(g[2][0], gc, g[2][1], A.inv_d2[2]);
+  const int h = A.halo;
+  const int c[3] = {i, j, k}, zone[3] = {ZX, ZY, ZZ};
+  T band = T(0);
+  bool in_band = false;
+#pragma unroll
+  for (int a = 0; a < ND; ++a) {
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+      if (zone[a] != 3 && zone[a] != s + 1) continue;
+      int q = c[a] - A.off[a][s];
+      if (zone[a] == 3 && (!A.active[a][s] || q < 0 || q > h + 1)) continue;
+      in_band = in_band || (q >= 1 && q <= h);
+      band += adj_side<T, I>(A, a, s, q, i, j, k, g[a][0], gc, g[a][1]);
+    }
+  }
+  adj_update<T, I, ND, GRAD>(A, o, l2, f, lap, band, in_band);
+}
+
+// Nodes of the shell boxes: a box's (x, y) columns numbered row by row,
+// l = (i - x0) + W (j - y0), in runs of 256 per block, one z plane per block;
+// the block's box kind selects the body.
+template <typename T, typename I, int ND, bool GRAD>
+__global__ void __launch_bounds__(256) adj_shell(const __grid_constant__ AdjStep<T> A) {
+  int b = 0;
+  const int blk = blockIdx.x;
+  while (b + 1 < A.nbox && blk >= A.box_blk[b + 1]) ++b;
+  const Box& B = A.box[b];
+  const int W = B.x1 - B.x0 + 1, ncol = W * (B.y1 - B.y0 + 1);
+  const int ncb = (ncol + 255) / 256;
+  const int r = blk - A.box_blk[b];
+  const int kz = r / ncb;
+  const int l = (r - kz * ncb) * 256 + threadIdx.x;
+  if (l >= ncol) return;
+  const int jl = l / W;
+  const int i = B.x0 + (l - jl * W), j = B.y0 + jl, k = ND == 3 ? B.z0 + kz : 0;
+#define AWC_SHELL(zx, zy, zz) \
+  case (zx) + 3 * (zy) + 9 * (zz): adj_shell_node<T, I, ND, GRAD, zx, zy, zz>(A, i, j, k); break;
+  if (ND == 2) {
+    switch (B.kind) {
+      AWC_SHELL(1, 0, 0) AWC_SHELL(2, 0, 0) AWC_SHELL(0, 1, 0) AWC_SHELL(1, 1, 0)
+      AWC_SHELL(2, 1, 0) AWC_SHELL(0, 2, 0) AWC_SHELL(1, 2, 0) AWC_SHELL(2, 2, 0)
+      default: adj_shell_node<T, I, ND, GRAD, 3, 3, 0>(A, i, j, k);
+    }
+  } else {
+    switch (B.kind) {
+      AWC_SHELL(1, 0, 0) AWC_SHELL(2, 0, 0) AWC_SHELL(0, 1, 0) AWC_SHELL(1, 1, 0)
+      AWC_SHELL(2, 1, 0) AWC_SHELL(0, 2, 0) AWC_SHELL(1, 2, 0) AWC_SHELL(2, 2, 0)
+      AWC_SHELL(0, 0, 1) AWC_SHELL(1, 0, 1) AWC_SHELL(2, 0, 1) AWC_SHELL(0, 1, 1)
+      AWC_SHELL(1, 1, 1) AWC_SHELL(2, 1, 1) AWC_SHELL(0, 2, 1) AWC_SHELL(1, 2, 1)
+      AWC_SHELL(2, 2, 1) AWC_SHELL(0, 0, 2) AWC_SHELL(1, 0, 2) AWC_SHELL(2, 0, 2)
+      AWC_SHELL(0, 1, 2) AWC_SHELL(1, 1, 2) AWC_SHELL(2, 1, 2) AWC_SHELL(0, 2, 2)
+      AWC_SHELL(1, 2, 2) AWC_SHELL(2, 2, 2)
+      default: adj_shell_node<T, I, ND, GRAD, 3, 3, 3>(A, i, j, k);
+    }
+  }
+#undef AWC_SHELL
+}
+
+// λ_{t+3} -= R_t at the receiver nodes before the step kernels run (the
+// residuals of step t enter λ_{t+1} = R_t + 2 λ_{t+2} - λ_{t+3} + ...), one
+// thread per node, its receivers in receiver order.
 template <typename T>
 __global__ void adj_residuals(T* __restrict__ lam3, const int64_t* __restrict__ node,
                               const int32_t* __restrict__ off, const int32_t* __restrict__ ids,
@@ -145,128 +302,6 @@ __global__ void adj_residuals(T* __restrict__ lam3, const int64_t* __restrict__ 
   T v = lam3[node[n]];
   for (int e = off[n]; e < off[n + 1]; ++e) v -= res_row[ids[e]];
   lam3[node[n]] = v;
-}
-
-// Whether node (i, j, k) lies in an active CPML band of any axis (where the
-// forward bracket holds ψ/ξ terms besides the Laplacian).
-template <typename T>
-__device__ __forceinline__ bool adj_in_band(const AdjParams<T>& A, int i, int j, int k) {
-  if (A.halo == 0) return false;
-  const int c[3] = {i, j, k}, n[3] = {A.nx, A.ny, A.nz};
-  for (int a = 0; a < A.ndim; ++a)
-    if ((A.active[a][0] && c[a] <= A.halo) || (A.active[a][1] && c[a] >= n[a] - A.halo - 1))
-      return true;
-  return false;
-}
-
-// λ_{t+1} = 2 λ_{t+2} - λ_{t+3} (residuals included, see adj_residuals) plus
-// the transposed stencil of G = F λ_{t+2} and the band terms, one thread per
-// node; then at the same node G = F λ_{t+1} for the next step and the
-// gradient accumulation dJ/dF += λ_{t+1} B_t: the Laplacian of p_t outside
-// the bands, (p_{t+1} - 2 p_t + p_{t-1}) / F inside them (where adj_sources
-// removes the source term).
-template <typename T>
-__global__ void __launch_bounds__(256) adj_lambda_grad(AdjParams<T> A, T* __restrict__ Gn,
-                                                       const T* __restrict__ pm1,
-                                                       const T* __restrict__ p0,
-                                                       const T* __restrict__ pp1,
-                                                       double* __restrict__ grad) {
-  const int i = 1 + blockIdx.x * 32 + threadIdx.x;
-  const int j = 1 + blockIdx.y * 8 + threadIdx.y;
-  const int k = A.ndim == 3 ? 1 + blockIdx.z : 0;
-  if (i > A.nx - 2 || j > A.ny - 2) return;
-  const int64_t px = A.px, plane = A.plane;
-  const int64_t o = i + px * j + plane * k;
-  const T gc = __ldg(A.G + o);
-  T lam = T(2) * __ldg(A.lam2 + o) - A.lam3[o];
-  lam += A.inv_d2[0] * (__ldg(A.G + o + 1) - T(2) * gc + __ldg(A.G + o - 1)) +
-         A.inv_d2[1] * (__ldg(A.G + o + px) - T(2) * gc + __ldg(A.G + o - px));
-  if (adj_band_near(A, i, A.nx)) lam += adj_band_terms(A, 0, i, A.nx, i, j, k);
-  if (adj_band_near(A, j, A.ny)) lam += adj_band_terms(A, 1, j, A.ny, i, j, k);
-  if (A.ndim == 3) {
-    lam += A.inv_d2[2] * (__ldg(A.G + o + plane) - T(2) * gc + __ldg(A.G + o - plane));
-    if (adj_band_near(A, k, A.nz)) lam += adj_band_terms(A, 2, k, A.nz, i, j, k);
-  }
-  A.lamn[o] = lam;
-  const T f = __ldg(A.F + o);
-  Gn[o] = f * lam;
-  if (grad) {
-    double b;
-    if (adj_in_band(A, i, j, k)) {
-      b = ((double)__ldg(pp1 + o) - 2.0 * (double)__ldg(p0 + o) + (double)__ldg(pm1 + o)) /
-          (double)f;
-    } else {
-      const double c = __ldg(p0 + o);
-      b = (double)A.inv_d2[0] * (((double)__ldg(p0 + o + 1) - 2.0 * c) + (double)__ldg(p0 + o - 1)) +
-          (double)A.inv_d2[1] * (((double)__ldg(p0 + o + px) - 2.0 * c) + (double)__ldg(p0 + o - px));
-      if (A.ndim == 3)
-        b += (double)A.inv_d2[2] *
-             (((double)__ldg(p0 + o + plane) - 2.0 * c) + (double)__ldg(p0 + o - plane));
-    }
-    grad[o] += (double)lam * b;
-  }
-}
-
-// The active band sides of one adjoint step, for one launch over all of
-// them: side n is axis ax[n], side sd[n], band nodes [start[n], start[n+1]).
-struct AdjSides {
-  int32_t n;
-  int32_t ax[6], sd[6];
-  int64_t start[7];
-};
-
-// ν_{t+1} and μ_{t+1} of every active side, one thread per band node (side,
-// entry q, other coordinates): ν_{t+1}[q-1] = bK ν_{t+2}[q-1] + F λ_{t+1};
-// face q (and face 0 for q = 1) of μ in place, with w of node q+1 formed from
-// ν_{t+2} so that no thread reads another's new ν. Sides touch disjoint
-// arrays.
-template <typename T>
-__global__ void __launch_bounds__(256) adj_band(AdjParams<T> A, AdjSides L) {
-  const int h = A.halo;
-  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < L.start[L.n];
-       g += (int64_t)gridDim.x * blockDim.x) {
-    int side = 0;
-    while (side + 1 < L.n && g >= L.start[side + 1]) ++side;
-    const int a = L.ax[side], s = L.sd[side];
-    const int64_t t = g - L.start[side];
-    const int n1 = a == 0 ? A.ny - 2 : A.nx - 2;  // fastest other coordinate count
-    int q, u, v;
-    if (a == 0) {  // q fastest: ψ_x is contiguous in q
-      q = 1 + (int)(t % h);
-      u = (int)((t / h) % n1);
-      v = (int)(t / ((int64_t)h * n1));
-    } else {       // x fastest
-      u = (int)(t % n1);
-      q = 1 + (int)((t / n1) % h);
-      v = (int)(t / ((int64_t)n1 * h));
-    }
-    const int c = q + A.off[a][s];
-    int i, j, k;
-    if (a == 0) { i = c; j = 1 + u; k = A.ndim == 3 ? 1 + v : 0; }
-    else if (a == 1) { i = 1 + u; j = c; k = A.ndim == 3 ? 1 + v : 0; }
-    else { i = 1 + u; j = 1 + v; k = c; }
-    const int64_t step = a == 0 ? 1 : a == 1 ? A.px : A.plane;
-    const int64_t o = i + A.px * j + A.plane * k;
-    const T flam = A.F[o] * A.lamn[o];
-    const int64_t x = band_index(A, a, h, q - 1, i, j, k);
-    const T nu_n = A.bK[a][s][q - 1] * A.nu_old[a][s][x] + flam;
-    A.nu_new[a][s][x] = nu_n;
-    const T wq = A.a[a][s][q - 1] * nu_n + flam;
-    T wn = 0;
-    if (q + 1 <= h) {
-      const int di = a == 0, dj = a == 1, dk = a == 2;
-      const T flam1 = A.F[o + step] * A.lamn[o + step];
-      const T nu1 = A.bK[a][s][q] * A.nu_old[a][s][band_index(A, a, h, q, i + di, j + dj, k + dk)] +
-                    flam1;
-      wn = A.a[a][s][q] * nu1 + flam1;
-    }
-    const int64_t m = band_index(A, a, h + 1, q, i, j, k);
-    A.mu[a][s][m] = A.bKh[a][s][q] * A.mu[a][s][m] + A.inv_d[a] * (wq - wn);
-    if (q == 1) {
-      const int64_t m0 = band_index(A, a, h + 1, 0, i, j, k);
-      A.mu[a][s][m0] = A.bKh[a][s][0] * A.mu[a][s][m0] - A.inv_d[a] * wq;
-    }
-  }
 }
 
 // Per source (one thread, serial over sources for a fixed summation order):
@@ -407,6 +442,113 @@ Groups group_nodes(const awc_problem* p, int64_t px, const int64_t* pos, int64_t
   return G;
 }
 
+// The adjoint's core box (nodes farther than one node from every active
+// band) and the shell boxes around it. Per axis the interior splits into the
+// left zone [1, h+1] (when the left side is active), the right zone
+// [n-h-2, n-2] (when the right one is) and the core range between them; the
+// shell is every product of zones but the core's (26 boxes in 3D, 8 in 2D),
+// each with its zone code as kind. When the zones of an axis leave no core
+// node between them, one generic box holds the whole interior.
+template <typename T>
+void adj_regions(awc::AdjStep<T>& A, int ndim) {
+  const int64_t n[3] = {A.nx, A.ny, A.nz}, h = A.halo;
+  int64_t lo[3][3], hi[3][3];  // [axis][zone]: 0 core, 1 left, 2 right
+  bool split = true;
+  for (int a = 0; a < 3; ++a) {
+    for (int z = 1; z < 3; ++z) {
+      lo[a][z] = 1;
+      hi[a][z] = 0;  // empty
+    }
+    if (a >= ndim) {
+      lo[a][0] = hi[a][0] = 0;
+      continue;
+    }
+    lo[a][0] = 1;
+    hi[a][0] = n[a] - 2;
+    if (A.active[a][0]) {
+      hi[a][1] = h + 1;
+      lo[a][0] = h + 2;
+    }
+    if (A.active[a][1]) {
+      lo[a][2] = n[a] - h - 2;
+      hi[a][2] = n[a] - 2;
+      hi[a][0] = n[a] - h - 3;
+    }
+    split = split && lo[a][0] <= hi[a][0];
+  }
+  A.nbox = 0;
+  auto add = [&](int zx, int zy, int zz, int32_t kind) {
+    if (lo[0][zx] > hi[0][zx] || lo[1][zy] > hi[1][zy] || lo[2][zz] > hi[2][zz]) return;
+    A.box[A.nbox++] = awc::Box{(int32_t)lo[0][zx], (int32_t)hi[0][zx], (int32_t)lo[1][zy],
+                               (int32_t)hi[1][zy], (int32_t)lo[2][zz], (int32_t)hi[2][zz], kind};
+  };
+  if (!split) {
+    A.core = awc::Box{1, 0, 1, 0, 0, 0, 0};  // none
+    for (int a = 0; a < ndim; ++a) {
+      lo[a][0] = 1;
+      hi[a][0] = n[a] - 2;
+    }
+    add(0, 0, 0, awc::ADJ_GENERIC);
+  } else {
+    A.core = awc::Box{(int32_t)lo[0][0], (int32_t)hi[0][0], (int32_t)lo[1][0],
+                      (int32_t)hi[1][0], (int32_t)lo[2][0], (int32_t)hi[2][0], 0};
+    for (int zz = 0; zz < (ndim == 3 ? 3 : 1); ++zz)
+      for (int zy = 0; zy < 3; ++zy)
+        for (int zx = 0; zx < 3; ++zx)
+          if (zx || zy || zz) add(zx, zy, zz, zx + 3 * zy + 9 * zz);
+  }
+  A.box_blk[0] = 0;
+  for (int b = 0; b < A.nbox; ++b) {
+    const awc::Box& B = A.box[b];
+    const int64_t ncol = (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
+    A.box_blk[b + 1] = (int32_t)(A.box_blk[b] + (ncol + 255) / 256 * (B.z1 - B.z0 + 1));
+  }
+  for (int b = A.nbox; b < 27; ++b) A.box_blk[b + 1] = A.box_blk[b];
+}
+
+// Offsets fit in int32 when every field (and so every band array) does.
+template <typename T, int ND, bool GRAD>
+void launch_core_i(const awc::AdjStep<T>& A, bool i64, dim3 grid, cudaStream_t st) {
+  if (i64)
+    awc::adj_core<T, int64_t, ND, GRAD><<<grid, dim3(32, 8), 0, st>>>(A);
+  else
+    awc::adj_core<T, int32_t, ND, GRAD><<<grid, dim3(32, 8), 0, st>>>(A);
+}
+
+template <typename T>
+void launch_core(const awc::AdjStep<T>& A, int ndim, bool grad, bool i64, dim3 grid,
+                 cudaStream_t st) {
+  if (ndim == 3 && grad)
+    launch_core_i<T, 3, true>(A, i64, grid, st);
+  else if (ndim == 3)
+    launch_core_i<T, 3, false>(A, i64, grid, st);
+  else if (grad)
+    launch_core_i<T, 2, true>(A, i64, grid, st);
+  else
+    launch_core_i<T, 2, false>(A, i64, grid, st);
+}
+
+template <typename T, int ND, bool GRAD>
+void launch_shell_i(const awc::AdjStep<T>& A, bool i64, unsigned blocks, cudaStream_t st) {
+  if (i64)
+    awc::adj_shell<T, int64_t, ND, GRAD><<<blocks, 256, 0, st>>>(A);
+  else
+    awc::adj_shell<T, int32_t, ND, GRAD><<<blocks, 256, 0, st>>>(A);
+}
+
+template <typename T>
+void launch_shell(const awc::AdjStep<T>& A, int ndim, bool grad, bool i64, unsigned blocks,
+                  cudaStream_t st) {
+  if (ndim == 3 && grad)
+    launch_shell_i<T, 3, true>(A, i64, blocks, st);
+  else if (ndim == 3)
+    launch_shell_i<T, 3, false>(A, i64, blocks, st);
+  else if (grad)
+    launch_shell_i<T, 2, true>(A, i64, blocks, st);
+  else
+    launch_shell_i<T, 2, false>(A, i64, blocks, st);
+}
+
 template <typename T>
 // Gradient mode (grad_out set): the checkpointed forward run gives the
 // traces, the misfit against `observed` and the residuals. Transpose mode
@@ -422,17 +564,13 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
   const bool want_grad = grad_out != nullptr;
   DevMem& mem = ctx_mem(C);
   // adjoint fields
-  T *lam[2], *G[2], *mu[3][2] = {}, *nu[3][2][2] = {};
-  for (int b = 0; b < 2; ++b) {
-    ADJ_TRY(C, mem.get(&lam[b], fb));
-    ADJ_TRY(C, mem.get(&G[b], fb));
-    ADJ_TRY(C, cudaMemsetAsync(G[b], 0, fb, st));
-  }
+  T *lam[2], *mu[3][2][2] = {}, *nu[3][2][2] = {};
+  for (int b = 0; b < 2; ++b) ADJ_TRY(C, mem.get(&lam[b], fb));
   for (int a = 0; a < p->ndim; ++a)
     for (int s = 0; s < 2; ++s) {
-      ADJ_TRY(C, mem.get(&mu[a][s], V.psi_len[a] * sizeof(T)));
-      ADJ_TRY(C, cudaMemsetAsync(mu[a][s], 0, std::max<int64_t>(V.psi_len[a], 1) * sizeof(T), st));
       for (int b = 0; b < 2; ++b) {
+        ADJ_TRY(C, mem.get(&mu[a][s][b], V.psi_len[a] * sizeof(T)));
+        ADJ_TRY(C, cudaMemsetAsync(mu[a][s][b], 0, std::max<int64_t>(V.psi_len[a], 1) * sizeof(T), st));
         ADJ_TRY(C, mem.get(&nu[a][s][b], V.xi_len[a] * sizeof(T)));
         ADJ_TRY(C, cudaMemsetAsync(nu[a][s][b], 0, std::max<int64_t>(V.xi_len[a], 1) * sizeof(T), st));
       }
@@ -490,8 +628,7 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
   ADJ_TRY(C, mem.get(&sband_d, sband.size()));
   ADJ_TRY(C, cudaMemcpyAsync(sband_d, sband.data(), sband.size(), cudaMemcpyHostToDevice, st));
   // kernel parameters
-  awc::AdjParams<T> A{};
-  A.ndim = p->ndim;
+  awc::AdjStep<T> A{};
   A.nx = (int32_t)p->nx;
   A.ny = (int32_t)p->ny;
   A.nz = (int32_t)V.nz;
@@ -513,30 +650,17 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       A.bK[a][s] = blk + 2 * h + s * h;
       A.ah[a][s] = blk + 4 * h + s * (h + 1);
       A.bKh[a][s] = blk + 4 * h + 2 * (h + 1) + s * (h + 1);
-      A.active[a][s] = V.active[a][s];
+      A.active[a][s] = h > 0 ? V.active[a][s] : 0;
       A.off[a][s] = s == 0 ? 0 : (int32_t)(n3[a] - h - 2);
-      A.mu[a][s] = mu[a][s];
     }
   }
-  // the active band sides, one launch per step over all of them
-  awc::AdjSides sides{};
-  sides.start[0] = 0;
-  for (int a = 0; a < p->ndim && h > 0; ++a)
-    for (int sd = 0; sd < 2; ++sd) {
-      if (!A.active[a][sd]) continue;
-      const int64_t n1 = a == 0 ? p->ny - 2 : p->nx - 2;
-      const int64_t n2 = p->ndim == 3 ? (a == 2 ? p->ny - 2 : V.nz - 2) : 1;
-      sides.ax[sides.n] = a;
-      sides.sd[sides.n] = sd;
-      sides.start[sides.n + 1] = sides.start[sides.n] + h * n1 * n2;
-      ++sides.n;
-    }
-  const unsigned band_blocks =
-      (unsigned)std::max<int64_t>(1, std::min<int64_t>((sides.start[sides.n] + 255) / 256,
-                                                       (int64_t)C->num_sms * 8));
-  const dim3 blk(32, 8);
-  const dim3 grid((unsigned)((p->nx - 2 + 31) / 32), (unsigned)((p->ny - 2 + 7) / 8),
-                  (unsigned)(p->ndim == 3 ? V.nz - 2 : 1));
+  adj_regions(A, p->ndim);
+  const bool has_core = A.core.x0 <= A.core.x1;
+  const dim3 core_grid((unsigned)((A.core.x1 - A.core.x0 + 32) / 32),
+                       (unsigned)((A.core.y1 - A.core.y0 + 8) / 8),
+                       (unsigned)(A.core.z1 - A.core.z0 + 1));
+  const unsigned shell_blocks = (unsigned)A.box_blk[A.nbox];
+  const bool i64 = NP > (int64_t)INT32_MAX;
   // checkpoints and segment fields (gradient only)
   const int64_t nseg = want_grad ? (nt + kchk - 1) / kchk : 0;
   int64_t band_elems = 0;
@@ -578,7 +702,7 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
     for (int64_t c = 0; c < nseg; ++c) {
       const int64_t s = c * kchk;
       if ((rc = save_or_restore(chk[c], s, true))) return rc;
-      if ((rc = awc_plan_run(plan, std::min(kchk, nt - s), 0, nullptr))) return rc;
+      if ((rc = awc_plan_run(plan, std::min(kchk, nt - s), 1, nullptr))) return rc;
     }
     res_h.assign(std::max<int64_t>(nt * nrec, 1), 0.0);
     if (nt * nrec > 0 && (rc = awc_plan_traces(plan, res_h.data()))) return rc;
@@ -596,7 +720,6 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
   ADJ_TRY(C, cudaMemcpyAsync(res_d, rows.data(), rows.size() * sizeof(T), cudaMemcpyHostToDevice, st));
   // backward
   int i2 = 0, i3 = 1;  // lam[i2] = λ_{t+2}, lam[i3] = λ_{t+3}
-  int gi = 0;          // G[gi] = F λ_{t+2}
   int par = 0;         // nu[..][par] holds ν_{t+2}
   for (int64_t c = (want_grad ? nseg : 1) - 1; c >= 0; --c) {
     const int64_t s = want_grad ? c * kchk : 0, e = want_grad ? std::min(s + kchk, nt) : nt;
@@ -607,39 +730,49 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       ADJ_TRY(C, cudaMemcpyAsync(seg[0], V.buf[s % 3], fb, cudaMemcpyDeviceToDevice, st));
       ADJ_TRY(C, cudaMemcpyAsync(seg[1], V.buf[(s + 1) % 3], fb, cudaMemcpyDeviceToDevice, st));
       awc::plan_keep_fields(plan, (void* const*)(seg.data() + 2), s, e - s);
-      rc = awc_plan_run(plan, e - s, 0, nullptr);
+      rc = awc_plan_run(plan, e - s, 1, nullptr);
       awc::plan_keep_fields(plan, nullptr, 0, 0);
       if (rc) return rc;
     }
     for (int64_t t = e - 1; t >= s; --t) {
-      // λ_{t+1} overwrites λ_{t+3}: adj_lambda_grad reads λ_{t+3} only at the
-      // node it writes
-      T* ln = lam[i3];
+      // λ_{t+1} overwrites λ_{t+3}, which the step kernels read only at the
+      // node they write
       A.lam2 = lam[i2];
-      A.lam3 = lam[i3];
-      A.lamn = ln;
-      A.G = G[gi];
+      A.lam = lam[i3];
       for (int a = 0; a < p->ndim; ++a)
         for (int sd = 0; sd < 2; ++sd) {
-          A.nu_old[a][sd] = nu[a][sd][par];
-          A.nu_new[a][sd] = nu[a][sd][par ^ 1];
+          A.nu_in[a][sd] = nu[a][sd][par];
+          A.nu_out[a][sd] = nu[a][sd][par ^ 1];
+          A.mu_in[a][sd] = mu[a][sd][par];
+          A.mu_out[a][sd] = mu[a][sd][par ^ 1];
         }
       if (!RG.node.empty())
         awc::adj_residuals<T><<<(unsigned)((RG.node.size() + 127) / 128), 128, 0, st>>>(
-            ln, rnode_d, roff_d, rids_d, (int32_t)RG.node.size(), res_d + t * nrec);
-      const T* pm1 = want_grad ? seg[t - s] : nullptr;
-      const T* p0 = want_grad ? seg[t - s + 1] : nullptr;
-      const T* pp1 = want_grad ? seg[t - s + 2] : nullptr;
-      awc::adj_lambda_grad<T><<<grid, blk, 0, st>>>(A, G[gi ^ 1], pm1, p0, pp1, grad);
+            A.lam, rnode_d, roff_d, rids_d, (int32_t)RG.node.size(), res_d + t * nrec);
+      A.pm1 = want_grad ? seg[t - s] : nullptr;
+      A.p0 = want_grad ? seg[t - s + 1] : nullptr;
+      A.pp1 = want_grad ? seg[t - s + 2] : nullptr;
+      A.grad = grad;
+      // the shell kernel on the second stream, the core kernel on the main one
+      const bool fork = has_core && shell_blocks > 0;
+      if (fork) {
+        ADJ_TRY(C, cudaEventRecord(C->ev_fork, st));
+        ADJ_TRY(C, cudaStreamWaitEvent(C->stream2, C->ev_fork, 0));
+      }
+      if (shell_blocks > 0)
+        launch_shell(A, p->ndim, want_grad, i64, shell_blocks, fork ? C->stream2 : st);
+      if (has_core) launch_core(A, p->ndim, want_grad, i64, core_grid, st);
+      if (fork) {
+        ADJ_TRY(C, cudaEventRecord(C->ev_join, C->stream2));
+        ADJ_TRY(C, cudaStreamWaitEvent(st, C->ev_join, 0));
+      }
       if (nsrc > 0)
-        awc::adj_sources<T><<<1, 32, 0, st>>>(ln, A.F, snode_d, sband_d, (int32_t)nsrc,
+        awc::adj_sources<T><<<1, 32, 0, st>>>(A.lam, A.F, snode_d, sband_d, (int32_t)nsrc,
                                               stf_d + t * nsrc, grad,
                                               sout_d ? sout_d + t * nsrc : nullptr);
-      if (sides.n > 0) awc::adj_band<T><<<band_blocks, 256, 0, st>>>(A, sides);
       ADJ_TRY(C, cudaGetLastError());
       std::swap(i2, i3);  // λ_{t+1} is the next step's λ_{t+2}
       par ^= 1;
-      gi ^= 1;
     }
   }
   // outputs
@@ -694,7 +827,8 @@ int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
   if (!observed || !grad_c2 || !misfit)
     return awc::fail(ctx, AWC_ERR_INVALID, "observed/grad_c2/misfit is NULL");
   if (checkpoint_every < 1) return awc::fail(ctx, AWC_ERR_INVALID, "checkpoint_every must be >= 1");
-  if ((rc = awc::plan_for(ctx, &ctx->adj_plan, p, vel, coeffs, possrcs, dt2srctf, posrecs)))
+  if ((rc = awc::plan_for(ctx, &ctx->adj_plan, p, vel, coeffs, possrcs, dt2srctf, posrecs,
+                          true)))
     return rc;
   awc_plan* plan = ctx->adj_plan;
   rc = p->precision == AWC_F64

@@ -306,8 +306,9 @@ struct awc_plan {
   int64_t step = 0;
   StepState state;
   int32_t active[3][2] = {};
-  // captured runs, by (first step, steps, state code at the first step)
-  std::map<std::array<int64_t, 3>, cudaGraphExec_t> graphs;
+  // captured runs, by (first step, steps, state code at the first step,
+  // first kept step, hash of the kept-field destinations; 0 without)
+  std::map<std::array<int64_t, 5>, cudaGraphExec_t> graphs;
   // Everything the captured kernel parameters hold by value besides the grid
   // shape and the fixed device buffers: the graphs are reused while it is
   // unchanged (a new shot of the same shape re-uploads data only).
@@ -1261,7 +1262,19 @@ int get_graph(awc_plan* P, int64_t start, int64_t n, cudaGraphExec_t* out) {
     P->drop_graphs();
     P->graph_key = key;
   }
-  const std::array<int64_t, 3> gk{start, n, P->state.code()};
+  // the field copies of a keep-fields run are part of the capture
+  int64_t kh = 0, kfirst = 0;
+  if (P->keep) {
+    kfirst = P->keep_first;
+    uint64_t hsh = 1469598103934665603ull;  // FNV-1a over the destinations in range
+    for (int64_t it = std::max(start, P->keep_first);
+         it < std::min(start + n, P->keep_first + P->keep_count); ++it) {
+      hsh ^= (uint64_t)(uintptr_t)P->keep[it - P->keep_first];
+      hsh *= 1099511628211ull;
+    }
+    kh = (int64_t)(hsh | 1);
+  }
+  const std::array<int64_t, 5> gk{start, n, P->state.code(), kfirst, kh};
   auto f = P->graphs.find(gk);
   if (f != P->graphs.end()) {
     *out = f->second;
@@ -1431,7 +1444,7 @@ PlanView plan_view(awc_plan* P) {
 
 int plan_for(awc_ctx* C, awc_plan** slot, const awc_problem* p, const double* vel,
              const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
-             const int64_t* posrecs) {
+             const int64_t* posrecs, bool tune) {
   awc_plan* P = *slot;
   if (P && p && p->ndim != 1 && !P->is1d && same_shape(P->p, *p)) {
     int rc;
@@ -1452,7 +1465,12 @@ int plan_for(awc_ctx* C, awc_plan** slot, const awc_problem* p, const double* ve
     awc_plan_destroy(P);
     *slot = nullptr;
   }
-  return awc_plan_create(C, p, vel, coeffs, possrcs, dt2srctf, posrecs, slot);
+  int rc = awc_plan_create(C, p, vel, coeffs, possrcs, dt2srctf, posrecs, slot);
+  if (rc || !tune || p->ndim != 3 || C->autotune_steps <= 0 || p->nt < 100) return rc;
+  P = *slot;
+  if ((rc = awc_plan_autotune(P, C->autotune_steps, nullptr))) return rc;
+  P->depth = 1;
+  return awc_plan_reset(P);
 }
 
 void plan_set_step(awc_plan* P, int64_t step) {
@@ -1658,7 +1676,6 @@ int awc_plan_run(awc_plan* P, int64_t nsteps, int32_t use_graph, float* ms) {
   if (n <= 0) return AWC_OK;
   int rc;
   if ((rc = prepare_launch(P))) return rc;
-  if (P->keep) use_graph = 0;  // field copies are made by eager runs only
   cudaGraphExec_t ex = nullptr;
   if (use_graph && (rc = get_graph(P, P->step, n, &ex))) return rc;
   CUDA_TRY(&C->err, cudaEventRecord(C->ev0, C->stream));

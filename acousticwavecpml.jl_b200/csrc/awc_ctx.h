@@ -57,10 +57,12 @@ void plan_set_step(awc_plan* P, int64_t step);
 void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count);
 
 // Re-uploads a new shot into *slot when it holds a plan of the same shape
-// (same buffers), else replaces it by a new plan. The plan is reset.
+// (same buffers), else replaces it by a new plan, whose 3D launch shape is
+// autotuned when `tune` is set (one-step passes either way). The plan is
+// reset.
 int plan_for(awc_ctx* C, awc_plan** slot, const awc_problem* p, const double* vel,
              const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
-             const int64_t* posrecs);
+             const int64_t* posrecs, bool tune = false);
 
 // Sets the calling thread's last error (awc_last_error(NULL)) and, when ctx
 // is not NULL, the context's; returns code.
