@@ -78,14 +78,18 @@ struct AdjStep {
   T* nu_out[3][2];       // ν_{t+2}
   const T* mu_in[3][2];  // μ_{t+3} (layout of ψ)
   T* mu_out[3][2];       // μ_{t+2}
-  const T* a[3][2];
-  const T* bK[3][2];
-  const T* ah[3][2];
-  const T* bKh[3][2];
+  // per axis and side: {bK_e, a_e} of the h on-grid entries and {bKh_f,
+  // ah_f} of the h + 1 half-grid faces, as pairs
+  const typename Vec2<T>::type* nuc[3][2];
+  const typename Vec2<T>::type* muc[3][2];
   int32_t active[3][2];
   int32_t off[3][2];     // band node c has entry q = c - off
-  // nodes farther than one node from every active band (the core kernel)
+  // nodes farther than one node from every active band (the core kernel);
+  // the TMA-fed core kernel tiles it from x = core_x (a 16-byte-aligned
+  // origin at or below core.x0) in z chunks of `zchunk` planes
   Box core;
+  int32_t core_x, zchunk;
+  int32_t* err;  // set to 1 when a bounded device wait runs out
   // disjoint boxes covering the other interior nodes (the shell kernel); box
   // b owns blocks [box_blk[b], box_blk[b+1]). Box.kind = zx + 3 zy + 9 zz
   // names the band zone of its nodes per axis (0 none, 1 next to or in the
@@ -123,11 +127,11 @@ __device__ __forceinline__ I band_step(const AdjStep<T>& A, int a) {
 template <typename T, typename I>
 __device__ __forceinline__ T adj_side(const AdjStep<T>& A, int a, int s, int q, int i, int j,
                                       int k, T gm, T gc, T gp) {
+  using V2 = typename Vec2<T>::type;
   const int h = A.halo;
   const I step = band_step<I>(A, a);
   const I nb = band_base<I>(A, a, h, i, j, k), mb = band_base<I>(A, a, h + 1, i, j, k);
-  const T* __restrict__ ca = A.a[a][s];
-  const T* __restrict__ cbK = A.bK[a][s];
+  const V2* __restrict__ nuc = A.nuc[a][s];
   const T* __restrict__ nu_in = A.nu_in[a][s];
   const T gv[3] = {gm, gc, gp};
   T w[3], anu[3];
@@ -137,28 +141,29 @@ __device__ __forceinline__ T adj_side(const AdjStep<T>& A, int a, int s, int q, 
     w[m] = T(0);
     anu[m] = T(0);
     if (e >= 0 && e < h) {
-      const T nu = fma(__ldg(cbK + e), __ldg(nu_in + nb + (I)e * step), gv[m]);
-      const T ae = __ldg(ca + e);
-      anu[m] = mul_rn(ae, nu);
-      w[m] = fma(ae, nu, gv[m]);
+      const V2 c = __ldg(nuc + e);  // {bK, a}
+      const T nu = fma(c.x, __ldg(nu_in + nb + (I)e * step), gv[m]);
+      anu[m] = mul_rn(c.y, nu);
+      w[m] = fma(c.y, nu, gv[m]);
       if (m == 1) A.nu_out[a][s][nb + (I)e * step] = nu;
     }
   }
   const T inv_d = A.inv_d[a];
-  const T* __restrict__ cbKh = A.bKh[a][s];
-  const T* __restrict__ cah = A.ah[a][s];
+  const V2* __restrict__ muc = A.muc[a][s];
   const T* __restrict__ mu_in = A.mu_in[a][s];
   T* __restrict__ mu_out = A.mu_out[a][s];
   T f = T(0);
   if (q >= 1) {  // face q - 1
     const int e = q - 1;
-    const T mu = fma(__ldg(cbKh + e), __ldg(mu_in + mb + (I)e * step), mul_rn(inv_d, w[0] - w[1]));
-    f = mul_rn(__ldg(cah + e), mu);
+    const V2 c = __ldg(muc + e);  // {bKh, ah}
+    const T mu = fma(c.x, __ldg(mu_in + mb + (I)e * step), mul_rn(inv_d, w[0] - w[1]));
+    f = mul_rn(c.y, mu);
     if (q == 1) mu_out[mb] = mu;
   }
   if (q <= h) {  // face q
-    const T mu = fma(__ldg(cbKh + q), __ldg(mu_in + mb + (I)q * step), mul_rn(inv_d, w[1] - w[2]));
-    f = f - mul_rn(__ldg(cah + q), mu);
+    const V2 c = __ldg(muc + q);
+    const T mu = fma(c.x, __ldg(mu_in + mb + (I)q * step), mul_rn(inv_d, w[1] - w[2]));
+    f = f - mul_rn(c.y, mu);
     if (q >= 1) mu_out[mb + (I)q * step] = mu;
   }
   const T acc = (anu[2] - T(2) * anu[1]) + anu[0];
@@ -185,7 +190,13 @@ __device__ __forceinline__ void adj_update(const AdjStep<T>& A, I o, T l2, T f, 
     const T c = __ldg(P + o);
     double b;
     if (in_band) {
-      b = (((double)__ldg(A.pp1 + o) - 2.0 * (double)c) + (double)__ldg(A.pm1 + o)) / (double)f;
+      // 1/F by Newton's iteration r <- r (2 - F r) from the single-precision
+      // reciprocal (two steps: ~1e-14, then below double rounding)
+      const double fd = (double)f;
+      double r = (double)__frcp_rn((float)fd);
+      r = r * fma(-fd, r, 2.0);
+      r = r * fma(-fd, r, 2.0);
+      b = (((double)__ldg(A.pp1 + o) - 2.0 * (double)c) + (double)__ldg(A.pm1 + o)) * r;
     } else {
       const I px = (I)A.px;
       T bl = second_diff(__ldg(P + o - 1), c, __ldg(P + o + 1), A.inv_d2[0]) +
@@ -254,7 +265,7 @@ __device__ __forceinline__ void adj_shell_node(const AdjStep<T>& A, int i, int j
 // l = (i - x0) + W (j - y0), in runs of 256 per block, one z plane per block;
 // the block's box kind selects the body.
 template <typename T, typename I, int ND, bool GRAD>
-__global__ void __launch_bounds__(256) adj_shell(const __grid_constant__ AdjStep<T> A) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) adj_shell(const __grid_constant__ AdjStep<T> A) {
   int b = 0;
   const int blk = blockIdx.x;
   while (b + 1 < A.nbox && blk >= A.box_blk[b + 1]) ++b;
@@ -288,6 +299,224 @@ __global__ void __launch_bounds__(256) adj_shell(const __grid_constant__ AdjStep
     }
   }
 #undef AWC_SHELL
+}
+
+// Geometry of the TMA-fed core kernel (32 x TY threads, a 64 x 2TY tile of
+// (x, y) nodes, 2 x 2 nodes per thread): one pipeline stage holds, for one z
+// plane, the boxes (64 + 2A) x (2TY + 2) around the tile of λ_{t+2}, F and
+// p_t (x apron A keeps the box origin 16-byte aligned), then the tile's
+// λ_{t+3} (64 x 2TY) and gradient (64 x 2TY doubles).
+template <typename T, int TY>
+struct AdjTile {
+  static constexpr int TX = 64;
+  static constexpr int RY = 2 * TY;
+  static constexpr int A = 16 / (int)sizeof(T);
+  static constexpr int PW = TX + 2 * A;
+  static constexpr int BOX = PW * (RY + 2) * (int)sizeof(T);
+  static constexpr int BOX_PAD = (BOX + 127) / 128 * 128;
+  static constexpr int IN_T = TX * RY * (int)sizeof(T);
+  static constexpr int IN_D = TX * RY * 8;
+  static constexpr int BYTES = 3 * BOX_PAD + IN_T + IN_D;
+};
+
+// The 2 x 2 values a thread reads from one box for its nodes and their x, y
+// neighbours: rows r0 (y = j0) and r1, x aprons, rows above and below.
+template <typename T>
+struct Quad {
+  typename Vec2<T>::type r0, r1, ym, yp;
+  T xm0, xp0, xm1, xp1;
+};
+template <typename T>
+__device__ __forceinline__ Quad<T> quad_at(const T* b, int c0, int pw) {
+  using V2 = typename Vec2<T>::type;
+  Quad<T> q;
+  q.r0 = *reinterpret_cast<const V2*>(b + c0);
+  q.r1 = *reinterpret_cast<const V2*>(b + c0 + pw);
+  q.ym = *reinterpret_cast<const V2*>(b + c0 - pw);
+  q.yp = *reinterpret_cast<const V2*>(b + c0 + 2 * pw);
+  q.xm0 = b[c0 - 1];
+  q.xp0 = b[c0 + 2];
+  q.xm1 = b[c0 + pw - 1];
+  q.xp1 = b[c0 + pw + 2];
+  return q;
+}
+// Element-wise product of two quads (G = F λ at the same points).
+template <typename T>
+__device__ __forceinline__ Quad<T> quad_mul(const Quad<T>& f, const Quad<T>& l) {
+  Quad<T> g;
+  g.r0 = {mul_rn(f.r0.x, l.r0.x), mul_rn(f.r0.y, l.r0.y)};
+  g.r1 = {mul_rn(f.r1.x, l.r1.x), mul_rn(f.r1.y, l.r1.y)};
+  g.ym = {mul_rn(f.ym.x, l.ym.x), mul_rn(f.ym.y, l.ym.y)};
+  g.yp = {mul_rn(f.yp.x, l.yp.x), mul_rn(f.yp.y, l.yp.y)};
+  g.xm0 = mul_rn(f.xm0, l.xm0);
+  g.xp0 = mul_rn(f.xp0, l.xp0);
+  g.xm1 = mul_rn(f.xm1, l.xm1);
+  g.xp1 = mul_rn(f.xp1, l.xp1);
+  return g;
+}
+// x + y second differences of a quad at its four nodes (00, 01, 10, 11), in
+// the order the per-node kernels use (x term + y term).
+template <typename T>
+__device__ __forceinline__ void quad_d2xy(const Quad<T>& q, T ix2, T iy2, T out[4]) {
+  out[0] = second_diff(q.xm0, q.r0.x, q.r0.y, ix2) + second_diff(q.ym.x, q.r0.x, q.r1.x, iy2);
+  out[1] = second_diff(q.r0.x, q.r0.y, q.xp0, ix2) + second_diff(q.ym.y, q.r0.y, q.r1.y, iy2);
+  out[2] = second_diff(q.xm1, q.r1.x, q.r1.y, ix2) + second_diff(q.r0.x, q.r1.x, q.yp.x, iy2);
+  out[3] = second_diff(q.r1.x, q.r1.y, q.xp1, ix2) + second_diff(q.r0.y, q.r1.y, q.yp.y, iy2);
+}
+
+// The core box streamed through shared memory: adj_core's arithmetic, node
+// for node, in the gradient mode, with λ_{t+2}, F, p_t (boxes with a ring),
+// λ_{t+3} and the gradient (the tile) staged by cp.async.bulk.tensor. Grid:
+// x tiles of 64 nodes from core_x, y tiles of 2TY rows from core.y0, z
+// chunks of `zchunk` planes from core.z0, numbered z chunk fastest. One
+// elected thread loads planes k0-1 .. k1 into S stages, each with a "full"
+// mbarrier (TMA bytes) and an "empty" one (one arrival per warp); plane k is
+// computed from the stages of k-1, k, k+1, and its λ_{t+1} and gradient are
+// stored as coalesced pairs. Every wait is bounded: on a timeout the block
+// records it in *A.err and drains its loads in flight.
+template <typename T, int TY, int S>
+__global__ void __launch_bounds__(32 * TY) adj_core_tma(const __grid_constant__ CUtensorMap ml,
+                                                        const __grid_constant__ CUtensorMap mf,
+                                                        const __grid_constant__ CUtensorMap mp,
+                                                        const __grid_constant__ CUtensorMap ml3,
+                                                        const __grid_constant__ CUtensorMap mg,
+                                                        const __grid_constant__ AdjStep<T> A) {
+  using L = AdjTile<T, TY>;
+  using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * L::BYTES);
+  uint64_t* empty = full + S;
+  volatile int* abort = reinterpret_cast<volatile int*>(empty + S);
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + 32 * ty;
+  const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  const Box C = A.core;
+  const int gz = gridDim.z, gx = gridDim.x;
+  const int bz = blk % gz, bx = (blk / gz) % gx, by = blk / (gz * gx);
+  const int x0 = A.core_x + bx * L::TX, y0 = C.y0 + by * L::RY;
+  const int k0 = C.z0 + bz * A.zchunk;
+  int k1 = k0 + A.zchunk;
+  if (k1 > C.z1 + 1) k1 = C.z1 + 1;
+  if (k0 >= k1) return;  // block-uniform
+  const int nplanes = k1 - k0 + 2;  // planes k0-1 .. k1
+
+  if (tid == 0) {
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], TY);
+    }
+    *abort = 0;
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto issue = [&](int u) {  // use u: plane k0 - 1 + u into stage u % S
+    const int s = u % S, m = k0 - 1 + u;
+    unsigned char* st = smem + s * L::BYTES;
+    const bool inner = m >= k0 && m < k1;
+    mbar_expect_tx(&full[s], 3 * L::BOX + (inner ? L::IN_T + L::IN_D : 0));
+    tma_load_3d(st, &ml, &full[s], x0 - L::A, y0 - 1, m);
+    tma_load_3d(st + L::BOX_PAD, &mf, &full[s], x0 - L::A, y0 - 1, m);
+    tma_load_3d(st + 2 * L::BOX_PAD, &mp, &full[s], x0 - L::A, y0 - 1, m);
+    if (inner) {
+      tma_load_3d(st + 3 * L::BOX_PAD, &ml3, &full[s], x0, y0, m);
+      tma_load_3d(st + 3 * L::BOX_PAD + L::IN_T, &mg, &full[s], x0, y0, m);
+    }
+  };
+  if (tid == 0)
+    for (int u = 0; u < S && u < nplanes; ++u) issue(u);
+
+  const int xa = x0 + 2 * tx, j0 = y0 + 2 * ty;
+  const bool vx0 = xa >= C.x0 && xa <= C.x1, vx1 = xa + 1 >= C.x0 && xa + 1 <= C.x1;
+  const bool vy0 = j0 <= C.y1, vy1 = j0 + 1 <= C.y1;
+  const bool all4 = vx0 && vx1 && vy0 && vy1;
+  const bool any = (vx0 || vx1) && vy0;
+  const int64_t px = A.px, plane = A.plane;
+  int64_t o = (int64_t)xa + px * j0 + plane * k0;
+  const int c0 = (2 * ty + 1) * L::PW + 2 * tx + L::A;  // box index of (xa, j0)
+  const int i0 = 2 * ty * L::TX + 2 * tx;               // tile index of (xa, j0)
+  const T ix2 = A.inv_d2[0], iy2 = A.inv_d2[1], iz2 = A.inv_d2[2];
+
+  bool ok = mbar_wait(&full[0], 0, abort) && mbar_wait(&full[1 % S], (1 / S) & 1, abort);
+  int uc = 1;
+  for (int k = k0; k < k1; ++k, ++uc, o += plane) {
+    ok = ok && mbar_wait(&full[(uc + 1) % S], ((uc + 1) / S) & 1, abort);
+    if (!ok) break;
+    const T* sm = reinterpret_cast<const T*>(smem + ((uc - 1) % S) * L::BYTES);
+    const T* sc = reinterpret_cast<const T*>(smem + (uc % S) * L::BYTES);
+    const T* sp = reinterpret_cast<const T*>(smem + ((uc + 1) % S) * L::BYTES);
+    constexpr int FO = L::BOX_PAD / (int)sizeof(T), PO = 2 * FO;  // F and p_t box offsets
+    // G = F λ on the plane and its two z neighbours
+    const Quad<T> lq = quad_at(sc, c0, L::PW);
+    const Quad<T> gq = quad_mul(quad_at(sc + FO, c0, L::PW), lq);
+    const V2 gm0 = {mul_rn(sm[FO + c0], sm[c0]), mul_rn(sm[FO + c0 + 1], sm[c0 + 1])};
+    const V2 gm1 = {mul_rn(sm[FO + c0 + L::PW], sm[c0 + L::PW]),
+                    mul_rn(sm[FO + c0 + L::PW + 1], sm[c0 + L::PW + 1])};
+    const V2 gp0 = {mul_rn(sp[FO + c0], sp[c0]), mul_rn(sp[FO + c0 + 1], sp[c0 + 1])};
+    const V2 gp1 = {mul_rn(sp[FO + c0 + L::PW], sp[c0 + L::PW]),
+                    mul_rn(sp[FO + c0 + L::PW + 1], sp[c0 + L::PW + 1])};
+    T lap[4];
+    quad_d2xy(gq, ix2, iy2, lap);
+    lap[0] += second_diff(gm0.x, gq.r0.x, gp0.x, iz2);
+    lap[1] += second_diff(gm0.y, gq.r0.y, gp0.y, iz2);
+    lap[2] += second_diff(gm1.x, gq.r1.x, gp1.x, iz2);
+    lap[3] += second_diff(gm1.y, gq.r1.y, gp1.y, iz2);
+    T b[4];
+    const Quad<T> pq = quad_at(sc + PO, c0, L::PW);
+    quad_d2xy(pq, ix2, iy2, b);
+    b[0] += second_diff(sm[PO + c0], pq.r0.x, sp[PO + c0], iz2);
+    b[1] += second_diff(sm[PO + c0 + 1], pq.r0.y, sp[PO + c0 + 1], iz2);
+    b[2] += second_diff(sm[PO + c0 + L::PW], pq.r1.x, sp[PO + c0 + L::PW], iz2);
+    b[3] += second_diff(sm[PO + c0 + L::PW + 1], pq.r1.y, sp[PO + c0 + L::PW + 1], iz2);
+    // the tile's λ_{t+3} and gradient of this plane
+    const T* l3s = reinterpret_cast<const T*>(smem + (uc % S) * L::BYTES + 3 * L::BOX_PAD);
+    const double* gs = reinterpret_cast<const double*>(smem + (uc % S) * L::BYTES +
+                                                       3 * L::BOX_PAD + L::IN_T);
+    const V2 a0 = *reinterpret_cast<const V2*>(l3s + i0);
+    const V2 a1 = *reinterpret_cast<const V2*>(l3s + i0 + L::TX);
+    const double2 q0 = *reinterpret_cast<const double2*>(gs + i0);
+    const double2 q1 = *reinterpret_cast<const double2*>(gs + i0 + L::TX);
+    // this warp is done with stage uc - 1
+    __syncwarp();
+    if (tx == 0) mbar_arrive(&empty[(uc - 1) % S]);
+    const T lam[4] = {(T(2) * lq.r0.x - a0.x) + (lap[0] + T(0)),
+                      (T(2) * lq.r0.y - a0.y) + (lap[1] + T(0)),
+                      (T(2) * lq.r1.x - a1.x) + (lap[2] + T(0)),
+                      (T(2) * lq.r1.y - a1.y) + (lap[3] + T(0))};
+    const double gr[4] = {q0.x + (double)lam[0] * (double)b[0], q0.y + (double)lam[1] * (double)b[1],
+                          q1.x + (double)lam[2] * (double)b[2], q1.y + (double)lam[3] * (double)b[3]};
+    if (all4) {
+      *reinterpret_cast<V2*>(A.lam + o) = V2{lam[0], lam[1]};
+      *reinterpret_cast<V2*>(A.lam + o + px) = V2{lam[2], lam[3]};
+      *reinterpret_cast<double2*>(A.grad + o) = double2{gr[0], gr[1]};
+      *reinterpret_cast<double2*>(A.grad + o + px) = double2{gr[2], gr[3]};
+    } else if (any) {
+      const bool v[4] = {vx0, vx1, vy1 && vx0, vy1 && vx1};
+      const int64_t off[4] = {0, 1, px, px + 1};
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        if (!v[n]) continue;
+        A.lam[o + off[n]] = lam[n];
+        A.grad[o + off[n]] = gr[n];
+      }
+    }
+    if (tid == 0 && uc - 1 + S < nplanes) {
+      if (!mbar_wait(&empty[(uc - 1) % S], ((uc - 1) / S) & 1, abort)) {
+        ok = false;
+        break;
+      }
+      issue(uc - 1 + S);
+    }
+  }
+  if (!ok) {
+    *abort = 1;
+    atomicExch(A.err, 1);
+    if (tid == 0) {
+      const int issued = nplanes < uc - 1 + S ? nplanes : uc - 1 + S;
+      for (int u = uc; u < issued; ++u) {
+        for (int n = 0; n < 64; ++n)
+          if (mbar_try_wait(&full[u % S], (u / S) & 1, 1000000u)) break;
+      }
+    }
+  }
 }
 
 // λ_{t+3} -= R_t at the receiver nodes before the step kernels run (the
@@ -549,14 +778,42 @@ void launch_shell(const awc::AdjStep<T>& A, int ndim, bool grad, bool i64, unsig
     launch_shell_i<T, 2, false>(A, i64, blocks, st);
 }
 
+// TMA-fed core kernel: tile 64 x 8 nodes, 4 stages.
+constexpr int ADJ_TY = 4, ADJ_STAGES = 4;
+template <typename T>
+constexpr int adj_core_smem() {
+  return ADJ_STAGES * awc::AdjTile<T, ADJ_TY>::BYTES + 2 * ADJ_STAGES * 8 + 16;
+}
+
+// Tensor map of a pitched field for the TMA core kernel's boxes.
+// Tensor map of a pitched field (elements of type E) for the TMA core
+// kernel: the box with a ring (ring = true) or the tile.
+template <typename T, typename E = T>
+bool adj_map(CUtensorMap* m, const void* base, const awc::PlanView& V, bool ring) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = awc::tensor_map_encoder();
+  if (!enc) return false;
+  using L = awc::AdjTile<T, ADJ_TY>;
+  const CUtensorMapDataType dt =
+      sizeof(E) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dims[3] = {(cuuint64_t)V.nx, (cuuint64_t)V.ny, (cuuint64_t)V.nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)(V.px * sizeof(E)),
+                                 (cuuint64_t)(V.px * V.ny * sizeof(E))};
+  const cuuint32_t box[3] = {ring ? (cuuint32_t)L::PW : (cuuint32_t)L::TX,
+                             (cuuint32_t)L::RY + (ring ? 2 : 0), 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return enc(m, dt, 3, const_cast<void*>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 template <typename T>
 // Gradient mode (grad_out set): the checkpointed forward run gives the
 // traces, the misfit against `observed` and the residuals. Transpose mode
 // (src_out set): `residual` are the adjoint traces.
-int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t* possrcs,
-                 const double* dt2srctf, const int64_t* posrecs, const double* residual,
-                 const double* observed, double* misfit, double* traces_out, int64_t kchk,
-                 double* grad_out, double* src_out) {
+int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double* coeffs,
+                 const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
+                 const double* residual, const double* observed, double* misfit,
+                 double* traces_out, int64_t kchk, double* grad_out, double* src_out) {
   const awc::PlanView V = awc::plan_view(plan);
   cudaStream_t st = V.stream;
   const int64_t nt = p->nt, nsrc = p->nsrc, nrec = p->nrec, h = p->halo;
@@ -641,15 +898,30 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
     A.inv_d2[a] = (T)(1.0 / (d[a] * d[a]));
   }
   A.F = (const T*)V.fact;
-  const T* cf = (const T*)V.coef;
   const int64_t n3[3] = {p->nx, p->ny, V.nz};
+  // coefficient pairs per axis and side: h {bK, a} then h + 1 {bKh, ah}, from
+  // the problem's coefficient vector (a_l a_r bK_l bK_r ah_l ah_r bKh_l bKh_r)
+  using V2 = typename awc::Vec2<T>::type;
+  const int64_t npair = 2 * h + 1;
+  std::vector<V2> pairs(std::max<int64_t>(p->ndim * 2 * npair, 1));
   for (int a = 0; a < p->ndim; ++a) {
-    const T* blk = cf + a * (8 * h + 4);
+    const double* blk = coeffs + a * (8 * h + 4);
     for (int s = 0; s < 2; ++s) {
-      A.a[a][s] = blk + s * h;
-      A.bK[a][s] = blk + 2 * h + s * h;
-      A.ah[a][s] = blk + 4 * h + s * (h + 1);
-      A.bKh[a][s] = blk + 4 * h + 2 * (h + 1) + s * (h + 1);
+      V2* pr = pairs.data() + (a * 2 + s) * npair;
+      for (int64_t e = 0; e < h; ++e)
+        pr[e] = V2{(T)blk[2 * h + s * h + e], (T)blk[s * h + e]};
+      for (int64_t f = 0; f <= h; ++f)
+        pr[h + f] = V2{(T)blk[4 * h + 2 * (h + 1) + s * (h + 1) + f], (T)blk[4 * h + s * (h + 1) + f]};
+    }
+  }
+  V2* pairs_d;
+  ADJ_TRY(C, mem.get(&pairs_d, pairs.size() * sizeof(V2)));
+  ADJ_TRY(C, cudaMemcpyAsync(pairs_d, pairs.data(), pairs.size() * sizeof(V2),
+                             cudaMemcpyHostToDevice, st));
+  for (int a = 0; a < p->ndim; ++a) {
+    for (int s = 0; s < 2; ++s) {
+      A.nuc[a][s] = pairs_d + (a * 2 + s) * npair;
+      A.muc[a][s] = pairs_d + (a * 2 + s) * npair + h;
       A.active[a][s] = h > 0 ? V.active[a][s] : 0;
       A.off[a][s] = s == 0 ? 0 : (int32_t)(n3[a] - h - 2);
     }
@@ -661,6 +933,29 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
                        (unsigned)(A.core.z1 - A.core.z0 + 1));
   const unsigned shell_blocks = (unsigned)A.box_blk[A.nbox];
   const bool i64 = NP > (int64_t)INT32_MAX;
+  // 3D gradient runs stream the core box through the TMA-fed kernel, in z
+  // chunks sized for about four waves of resident blocks
+  using Tile = awc::AdjTile<T, ADJ_TY>;
+  A.err = V.err_flag;
+  A.core_x = (int32_t)(A.core.x0 / Tile::A * Tile::A);
+  bool use_tma = p->ndim == 3 && want_grad && has_core && awc::tensor_map_encoder() != nullptr;
+  dim3 tma_grid;
+  if (use_tma) {
+    const int64_t gx = (A.core.x1 + 1 - A.core_x + Tile::TX - 1) / Tile::TX;
+    const int64_t gy = (A.core.y1 - A.core.y0 + Tile::RY) / Tile::RY;
+    const int64_t nzc = A.core.z1 - A.core.z0 + 1;
+    int per_sm = 0;
+    ADJ_TRY(C, cudaFuncSetAttribute(awc::adj_core_tma<T, ADJ_TY, ADJ_STAGES>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    adj_core_smem<T>()));
+    ADJ_TRY(C, cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                   &per_sm, awc::adj_core_tma<T, ADJ_TY, ADJ_STAGES>, 32 * ADJ_TY,
+                   adj_core_smem<T>()));
+    const int64_t target = 4 * (int64_t)C->num_sms * std::max(per_sm, 1);
+    const int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(nzc, target / (gx * gy)));
+    A.zchunk = (int32_t)std::max<int64_t>(4, (nzc + chunks - 1) / chunks);
+    tma_grid = dim3((unsigned)gx, (unsigned)gy, (unsigned)((nzc + A.zchunk - 1) / A.zchunk));
+  }
   // checkpoints and segment fields (gradient only)
   const int64_t nseg = want_grad ? (nt + kchk - 1) / kchk : 0;
   int64_t band_elems = 0;
@@ -675,6 +970,17 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
     ADJ_TRY(C, mem.get(&arena, (nseg * chk_elems + (int64_t)seg.size() * NP) * sizeof(T)));
     for (int64_t c = 0; c < nseg; ++c) chk[c] = arena + c * chk_elems;
     for (size_t m = 0; m < seg.size(); ++m) seg[m] = arena + nseg * chk_elems + (int64_t)m * NP;
+  }
+  // tensor maps of the TMA-fed core kernel: both λ buffers, F, every segment field
+  CUtensorMap map_lam[2], map_lam3[2], map_f, map_grad;
+  std::vector<CUtensorMap> map_seg(seg.size());
+  if (use_tma) {
+    use_tma = adj_map<T>(&map_lam[0], lam[0], V, true) && adj_map<T>(&map_lam[1], lam[1], V, true) &&
+              adj_map<T>(&map_lam3[0], lam[0], V, false) &&
+              adj_map<T>(&map_lam3[1], lam[1], V, false) && adj_map<T>(&map_f, V.fact, V, true) &&
+              adj_map<T, double>(&map_grad, grad, V, false);
+    for (size_t m = 0; use_tma && m < seg.size(); ++m)
+      use_tma = adj_map<T>(&map_seg[m], seg[m], V, true);
   }
   auto save_or_restore = [&](T* base, int64_t s, bool save) -> int {
     auto cp = [&](void* dst, const void* src, size_t bytes) {
@@ -761,7 +1067,13 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
       }
       if (shell_blocks > 0)
         launch_shell(A, p->ndim, want_grad, i64, shell_blocks, fork ? C->stream2 : st);
-      if (has_core) launch_core(A, p->ndim, want_grad, i64, core_grid, st);
+      if (has_core && use_tma) {
+        awc::adj_core_tma<T, ADJ_TY, ADJ_STAGES>
+            <<<tma_grid, dim3(32, ADJ_TY), adj_core_smem<T>(), st>>>(
+                map_lam[i2], map_f, map_seg[t - s + 1], map_lam3[i3], map_grad, A);
+      } else if (has_core) {
+        launch_core(A, p->ndim, want_grad, i64, core_grid, st);
+      }
       if (fork) {
         ADJ_TRY(C, cudaEventRecord(C->ev_join, C->stream2));
         ADJ_TRY(C, cudaStreamWaitEvent(st, C->ev_join, 0));
@@ -797,7 +1109,13 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const int64_t
     for (int64_t s2 = 0; s2 < nsrc; ++s2)
       for (int64_t t = 0; t < nt; ++t) src_out[t + nt * s2] = tmp[t * nsrc + s2];
   }
+  int32_t flag = 0;
+  ADJ_TRY(C, cudaMemcpyAsync(&flag, V.err_flag, 4, cudaMemcpyDeviceToHost, st));
   ADJ_TRY(C, cudaStreamSynchronize(st));
+  if (flag) {
+    ADJ_TRY(C, cudaMemsetAsync(V.err_flag, 0, 4, st));
+    return awc::fail(C, AWC_ERR_TIMEOUT, "a bounded wait on a pipeline barrier ran out");
+  }
   return AWC_OK;
 }
 
@@ -832,10 +1150,10 @@ int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
     return rc;
   awc_plan* plan = ctx->adj_plan;
   rc = p->precision == AWC_F64
-           ? adjoint_impl<double>(ctx, plan, p, possrcs, dt2srctf, posrecs, nullptr, observed,
-                                  misfit, traces, checkpoint_every, grad_c2, nullptr)
-           : adjoint_impl<float>(ctx, plan, p, possrcs, dt2srctf, posrecs, nullptr, observed,
-                                 misfit, traces, checkpoint_every, grad_c2, nullptr);
+           ? adjoint_impl<double>(ctx, plan, p, coeffs, possrcs, dt2srctf, posrecs, nullptr,
+                                  observed, misfit, traces, checkpoint_every, grad_c2, nullptr)
+           : adjoint_impl<float>(ctx, plan, p, coeffs, possrcs, dt2srctf, posrecs, nullptr,
+                                 observed, misfit, traces, checkpoint_every, grad_c2, nullptr);
   return rc;
 }
 
@@ -854,10 +1172,10 @@ int awc_adjoint_sources(awc_ctx* ctx, const awc_problem* p, const double* vel,
     return rc;
   awc_plan* plan = ctx->adj_plan;
   rc = p->precision == AWC_F64
-           ? adjoint_impl<double>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces,
-                                  nullptr, nullptr, nullptr, 1, nullptr, src_out)
-           : adjoint_impl<float>(ctx, plan, p, possrcs, nullptr, posrecs, adjoint_traces,
-                                 nullptr, nullptr, nullptr, 1, nullptr, src_out);
+           ? adjoint_impl<double>(ctx, plan, p, coeffs, possrcs, nullptr, posrecs,
+                                  adjoint_traces, nullptr, nullptr, nullptr, 1, nullptr, src_out)
+           : adjoint_impl<float>(ctx, plan, p, coeffs, possrcs, nullptr, posrecs,
+                                 adjoint_traces, nullptr, nullptr, nullptr, 1, nullptr, src_out);
   return rc;
 }
 

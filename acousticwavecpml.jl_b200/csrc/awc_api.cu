@@ -1438,6 +1438,7 @@ PlanView plan_view(awc_plan* P) {
   }
   V.coef = P->coef;
   V.traces = P->traces;
+  V.err_flag = P->err_flag;
   V.stream = P->ctx->stream;
   return V;
 }

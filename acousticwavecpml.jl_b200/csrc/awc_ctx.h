@@ -47,6 +47,7 @@ struct PlanView {
   const void* coef = nullptr;               // packed coefficients in the working precision
   int32_t active[3][2] = {};
   const void* traces = nullptr;             // device [nt][nrec]
+  int32_t* err_flag = nullptr;              // device flag of timed-out bounded waits
   cudaStream_t stream = nullptr;
 };
 PlanView plan_view(awc_plan* P);
