@@ -128,7 +128,7 @@ def test_fp32_gradient_follows_fp64(pkg, ctx, dim):
     J32, g32, _ = adjoint.misfit_gradient(s32, obs, 25, ctx)
     e = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
     print(f"{dim}D fp32 gradient rel-L2 {e:.3e}, misfit {J32:.6e} vs {J64:.6e}")
-    assert e <= 2e-3
+    assert e <= 1e-4
     assert abs(J32 - J64) <= 1e-4 * J64
 
 

@@ -209,5 +209,5 @@ def test_config4_fp32_gradient_two_shots(pkg, ctx, config4):
     e = cases.rel_l2(g["f32"], g["f64"])
     print(f"config4 two shots: FP32 vs FP64 gradient rel-L2 {e:.3e}, misfit "
           f"{J['f32']:.8e} vs {J['f64']:.8e}")
-    assert e <= 1e-3
+    assert e <= 3e-4
     assert abs(J["f32"] - J["f64"]) <= 1e-4 * J["f64"]
