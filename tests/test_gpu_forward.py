@@ -246,6 +246,49 @@ def test_forward_reuses_cached_plan(pkg, oracle, ctx):
     assert cases.rel_l2(a[1][1], b[1][1]) > 1e-6
 
 
+def _shot3d(d, freetop, srcs, recs, seed):
+    """small3d's 40 x 34 x 28 grid with node spacing d."""
+    nx, ny, nz = 40, 34, 28
+    rng = np.random.default_rng(seed)
+    vel = 2000.0 + 15.0 * np.arange(ny)[None, :, None] + 50.0 * rng.random((nx, ny, nz))
+    L = ((nx - 1) * d, (ny - 1) * d, (nz - 1) * d)
+    to_m = lambda pts: [[c * d for c in q] for q in pts]  # noqa: E731 (node index -> m)
+    return (L, 0.2 * d / 10.0, vel, to_m(srcs), [0.05] * len(srcs), 12.0, to_m(recs),
+            dict(halo=6, rcoef=1e-4, freetop=freetop, check_ppw=False))
+
+
+def test_cached_graphs_follow_changed_inputs(pkg, oracle, ctx):
+    """Shots of one shape in sequence through awc_forward, which keeps the
+    plan and its CUDA graph while nothing the kernel parameters hold by value
+    changes: the free top (live band sides), the spacing, and the
+    source/receiver lists (with rim sources, so the rim list changes) vary
+    from shot to shot; every result must follow its own inputs."""
+    recs = [[2, 3, 3], [20, 3, 14], [37, 30, 24]]
+    shots3d = [
+        _shot3d(10.0, True, [[20, 8, 14]], recs, 1),
+        _shot3d(10.0, False, [[20, 8, 14]], recs, 1),            # live sides change
+        _shot3d(12.0, False, [[20, 8, 14]], recs, 1),            # spacing changes
+        _shot3d(12.0, False, [[10, 0, 10], [21, 9, 13]], recs + [[10, 0, 10]], 2),  # rim
+        _shot3d(12.0, False, [[21, 9, 13]] * 2, recs[:1], 3),    # back to no rim I/O
+    ]
+    shots2d = [((400.0, 300.0), 0.3, 2000.0 * np.ones((41, 31)), sp, [0.1] * len(sp), 10.0, rp,
+                dict(halo=5, freetop=ft, check_ppw=False))
+               for sp, rp, ft in (([[200.0, 150.0]], [[100.0, 100.0]], True),
+                                  ([[200.0, 150.0]], [[100.0, 100.0]], False),
+                                  ([[0.0, 150.0], [120.0, 80.0]], [[0.0, 150.0], [300.0, 20.0]],
+                                   False),
+                                  ([[120.0, 80.0]], [[300.0, 20.0]], True))]
+    for case in shots3d + shots2d:
+        for precision in ("f64", "f32"):
+            _, (pend, traces), (pend_o, traces_o) = run_both(pkg, oracle, ctx, case, precision)
+            assert np.abs(traces_o).max() > 0
+            if precision == "f64":
+                assert cases.rel_l2(traces, traces_o) <= TOL64
+                assert cases.rel_l2(pend, pend_o) <= TOL64
+            else:
+                assert cases.rel_l2(traces, traces_o) <= TOL32
+
+
 def test_solve2D_api_golden(pkg):
     from acousticwavecpml_b200.Acoustic2D_CUDA import solve2D
     lengths, lt, vel, sp, t0s, f0, rp, kw = cases.ref_gradient()
