@@ -1095,7 +1095,7 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
     const int blocks = (int)std::min<int64_t>((N + 255) / 256, (int64_t)C->num_sms * 16);
     awc::scale_unpitch<<<blocks, 256, 0, st>>>(grad, dense, N, p->nx, V.px, p->dt * p->dt);
     ADJ_TRY(C, cudaGetLastError());
-    ADJ_TRY(C, cudaMemcpyAsync(grad_out, dense, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ADJ_TRY(C, awc::copy_to_host(C, grad_out, dense, N * sizeof(double), st));
   }
   if (src_out && nsrc > 0) {
     double* sd;

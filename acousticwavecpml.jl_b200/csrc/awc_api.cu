@@ -20,6 +20,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -372,6 +373,72 @@ struct awc_plan {
   }
 };
 
+namespace awc {
+namespace {
+// A host buffer is pinned when the runtime knows it as host memory.
+bool is_pinned(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+// memcpy split over up to 8 threads (one 8 MB slice per thread at least).
+void host_copy(void* dst, const void* src, size_t bytes) {
+  const size_t nth = std::max<size_t>(
+      1, std::min<size_t>({8, (size_t)std::max(1u, std::thread::hardware_concurrency()),
+                           bytes / (8u << 20)}));
+  if (nth == 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t chunk = (bytes + nth - 1) / nth;
+  for (size_t t = 0; t < nth; ++t) {
+    const size_t a = t * chunk, b = std::min(bytes, a + chunk);
+    if (a >= b) break;
+    th.emplace_back([=]() { std::memcpy((char*)dst + a, (const char*)src + a, b - a); });
+  }
+  for (auto& x : th) x.join();
+}
+cudaError_t stage(awc_ctx* C, size_t bytes) {
+  if (C->host_stage_bytes >= bytes) return cudaSuccess;
+  if (C->host_stage) cudaFreeHost(C->host_stage);
+  C->host_stage = nullptr;
+  C->host_stage_bytes = 0;
+  cudaError_t e = cudaMallocHost(&C->host_stage, bytes);
+  if (e == cudaSuccess) C->host_stage_bytes = bytes;
+  return e;
+}
+constexpr size_t kStageMin = 16u << 20;  // smaller copies go directly
+}  // namespace
+
+cudaError_t copy_to_device(awc_ctx* C, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  cudaError_t e;
+  if (bytes < kStageMin || is_pinned(src) || stage(C, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  } else {
+    host_copy(C->host_stage, src, bytes);
+    e = cudaMemcpyAsync(dst, C->host_stage, bytes, cudaMemcpyHostToDevice, st);
+  }
+  return e != cudaSuccess ? e : cudaStreamSynchronize(st);
+}
+
+cudaError_t copy_to_host(awc_ctx* C, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (bytes < kStageMin || is_pinned(dst) || stage(C, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st);
+    return e != cudaSuccess ? e : cudaStreamSynchronize(st);
+  }
+  cudaError_t e = cudaMemcpyAsync(C->host_stage, src, bytes, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) host_copy(dst, C->host_stage, bytes);
+  return e;
+}
+}  // namespace awc
+
 namespace {
 
 // Elements of one band layer of axis `axis`: ψ/ξ of axis x are
@@ -453,6 +520,7 @@ int grid_for(const awc_ctx* C, int64_t n, int threads) {
                                                      (int64_t)C->num_sms * 16));
 }
 
+
 void make_regions(awc_plan* P);
 void box_blocks(awc_plan* P);
 bool tb_eligible(const awc_plan* P);
@@ -468,7 +536,7 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
   const int64_t h = p->halo, nt = p->nt, nsrc = p->nsrc, nrec = p->nrec;
   const bool f64 = p->precision == AWC_F64;
   // fact = dt^2 vel^2 on the device in FP64, written pitched
-  CUDA_TRY(err, cudaMemcpyAsync(P->staging, vel, P->N * 8, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(err, awc::copy_to_device(C, P->staging, vel, P->N * 8, st));
   {
     const double dt2 = p->dt * p->dt;
     const int blocks = grid_for(C, P->N, 256);
@@ -1593,6 +1661,7 @@ void awc_destroy(awc_ctx* ctx) {
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
   delete ctx;
 }
 
@@ -1808,8 +1877,7 @@ int awc_plan_traces(awc_plan* P, double* traces) {
   else
     awc::traces_out<float><<<grid, dim3(32, 8), 0, C->stream>>>((const float*)P->traces, P->staging, nt, nrec);
   CUDA_TRY(&C->err, cudaGetLastError());
-  CUDA_TRY(&C->err, cudaMemcpyAsync(traces, P->staging, nt * nrec * 8, cudaMemcpyDeviceToHost, C->stream));
-  CUDA_TRY(&C->err, cudaStreamSynchronize(C->stream));
+  CUDA_TRY(&C->err, awc::copy_to_host(C, traces, P->staging, nt * nrec * 8, C->stream));
   return AWC_OK;
 }
 
@@ -1826,8 +1894,7 @@ int awc_plan_field(awc_plan* P, double* out) {
   else
     awc::unpitch<float><<<blocks, 256, 0, C->stream>>>((const float*)cur, P->staging, n, P->p.nx, P->px);
   CUDA_TRY(&C->err, cudaGetLastError());
-  CUDA_TRY(&C->err, cudaMemcpyAsync(out, P->staging, n * 8, cudaMemcpyDeviceToHost, C->stream));
-  CUDA_TRY(&C->err, cudaStreamSynchronize(C->stream));
+  CUDA_TRY(&C->err, awc::copy_to_host(C, out, P->staging, n * 8, C->stream));
   return AWC_OK;
 }
 

@@ -29,6 +29,9 @@ struct awc_ctx {
   awc_plan* adj_plan = nullptr;
   void* adj_mem = nullptr;
   std::function<void()> adj_release;
+  // pinned host staging buffer for large pageable copies (grown on demand)
+  void* host_stage = nullptr;
+  size_t host_stage_bytes = 0;
 };
 
 namespace awc {
@@ -64,6 +67,13 @@ void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t coun
 int plan_for(awc_ctx* C, awc_plan** slot, const awc_problem* p, const double* vel,
              const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
              const int64_t* posrecs, bool tune = false);
+
+// Host <-> device copies that return once complete. Large pageable host
+// buffers go through the context's pinned staging buffer, the host side of
+// the copy split over several threads; pinned buffers and small copies go
+// directly.
+cudaError_t copy_to_device(awc_ctx* C, void* dst, const void* src, size_t bytes, cudaStream_t st);
+cudaError_t copy_to_host(awc_ctx* C, void* dst, const void* src, size_t bytes, cudaStream_t st);
 
 // Sets the calling thread's last error (awc_last_error(NULL)) and, when ctx
 // is not NULL, the context's; returns code.
