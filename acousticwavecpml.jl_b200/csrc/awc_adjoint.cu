@@ -806,6 +806,17 @@ bool adj_map(CUtensorMap* m, const void* base, const awc::PlanView& V, bool ring
              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// The adjoint's two streams and five events of the context (created once).
+int adj_streams(awc_ctx* C, cudaStream_t* a, cudaStream_t* b) {
+  for (cudaStream_t& s : C->adj_stream)
+    if (!s) ADJ_TRY(C, cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  for (cudaEvent_t& e : C->adj_ev)
+    if (!e) ADJ_TRY(C, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  *a = C->adj_stream[0];
+  *b = C->adj_stream[1];
+  return AWC_OK;
+}
+
 template <typename T>
 // Gradient mode (grad_out set): the checkpointed forward run gives the
 // traces, the misfit against `observed` and the residuals. Transpose mode
@@ -961,26 +972,36 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
   int64_t band_elems = 0;
   for (int a = 0; a < p->ndim; ++a) band_elems += 2 * (V.psi_len[a] + V.xi_len[a]);
   std::vector<T*> chk(nseg, nullptr);
-  std::vector<T*> seg;
+  // segment fields: two sets, so that segment c - 1 is recomputed into one
+  // while the backward steps of segment c read the other
+  const int nset = nseg > 1 ? 2 : 1;
+  std::vector<T*> seg[2];
   if (want_grad) {
-    // one allocation for the saved states and the segment's fields
+    // one allocation for the saved states and the segments' fields
     const int64_t chk_elems = (3 * NP + band_elems + 63) / 64 * 64;
-    seg.resize(std::min<int64_t>(kchk, nt) + 2);
+    const int64_t nfield = std::min<int64_t>(kchk, nt) + 2;
     T* arena;
-    ADJ_TRY(C, mem.get(&arena, (nseg * chk_elems + (int64_t)seg.size() * NP) * sizeof(T)));
+    ADJ_TRY(C, mem.get(&arena, (nseg * chk_elems + nset * nfield * NP) * sizeof(T)));
     for (int64_t c = 0; c < nseg; ++c) chk[c] = arena + c * chk_elems;
-    for (size_t m = 0; m < seg.size(); ++m) seg[m] = arena + nseg * chk_elems + (int64_t)m * NP;
+    for (int b = 0; b < nset; ++b) {
+      seg[b].resize(nfield);
+      for (int64_t m = 0; m < nfield; ++m)
+        seg[b][m] = arena + nseg * chk_elems + (b * nfield + m) * NP;
+    }
   }
   // tensor maps of the TMA-fed core kernel: both λ buffers, F, every segment field
   CUtensorMap map_lam[2], map_lam3[2], map_f, map_grad;
-  std::vector<CUtensorMap> map_seg(seg.size());
+  std::vector<CUtensorMap> map_seg[2];
   if (use_tma) {
     use_tma = adj_map<T>(&map_lam[0], lam[0], V, true) && adj_map<T>(&map_lam[1], lam[1], V, true) &&
               adj_map<T>(&map_lam3[0], lam[0], V, false) &&
               adj_map<T>(&map_lam3[1], lam[1], V, false) && adj_map<T>(&map_f, V.fact, V, true) &&
               adj_map<T, double>(&map_grad, grad, V, false);
-    for (size_t m = 0; use_tma && m < seg.size(); ++m)
-      use_tma = adj_map<T>(&map_seg[m], seg[m], V, true);
+    for (int b = 0; b < nset; ++b) {
+      map_seg[b].resize(seg[b].size());
+      for (size_t m = 0; use_tma && m < seg[b].size(); ++m)
+        use_tma = adj_map<T>(&map_seg[b][m], seg[b][m], V, true);
+    }
   }
   auto save_or_restore = [&](T* base, int64_t s, bool save) -> int {
     auto cp = [&](void* dst, const void* src, size_t bytes) {
@@ -1024,22 +1045,39 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
   for (int64_t r = 0; r < nrec; ++r)
     for (int64_t t = 0; t < nt; ++t) rows[t * nrec + r] = (T)residual[t + nt * r];
   ADJ_TRY(C, cudaMemcpyAsync(res_d, rows.data(), rows.size() * sizeof(T), cudaMemcpyHostToDevice, st));
-  // backward
+  // backward: the steps run on the adjoint's two streams (core kernel on the
+  // first, shell kernel on the second); segment c - 1 is recomputed on the
+  // plan's stream into the other field set meanwhile
+  cudaStream_t bs = nullptr, bs2 = nullptr;
+  if ((rc = adj_streams(C, &bs, &bs2))) return rc;
+  cudaEvent_t ev_fork = C->adj_ev[0], ev_join = C->adj_ev[1], ev_rec = C->adj_ev[2];
+  cudaEvent_t* ev_free = C->adj_ev + 3;  // set b's backward steps are done
+  ADJ_TRY(C, cudaEventRecord(ev_rec, st));  // the set-up above
+  ADJ_TRY(C, cudaStreamWaitEvent(bs, ev_rec, 0));
+  auto recompute = [&](int64_t c) -> int {
+    // p_{s-1} .. p_e of segment c into field set c % 2
+    const int64_t s = c * kchk, e = std::min(s + kchk, nt);
+    const int b = (int)(c % nset);
+    if (c + nset <= nseg - 1) ADJ_TRY(C, cudaStreamWaitEvent(st, ev_free[b], 0));
+    int r;
+    if ((r = save_or_restore(chk[c], s, false))) return r;
+    awc::plan_set_step(plan, s);
+    ADJ_TRY(C, cudaMemcpyAsync(seg[b][0], V.buf[s % 3], fb, cudaMemcpyDeviceToDevice, st));
+    ADJ_TRY(C, cudaMemcpyAsync(seg[b][1], V.buf[(s + 1) % 3], fb, cudaMemcpyDeviceToDevice, st));
+    awc::plan_keep_fields(plan, (void* const*)(seg[b].data() + 2), s, e - s);
+    r = awc_plan_run(plan, e - s, 1, nullptr);
+    awc::plan_keep_fields(plan, nullptr, 0, 0);
+    if (r) return r;
+    ADJ_TRY(C, cudaEventRecord(ev_rec, st));
+    return AWC_OK;
+  };
   int i2 = 0, i3 = 1;  // lam[i2] = λ_{t+2}, lam[i3] = λ_{t+3}
   int par = 0;         // nu[..][par] holds ν_{t+2}
+  if (want_grad && (rc = recompute(nseg - 1))) return rc;
   for (int64_t c = (want_grad ? nseg : 1) - 1; c >= 0; --c) {
     const int64_t s = want_grad ? c * kchk : 0, e = want_grad ? std::min(s + kchk, nt) : nt;
-    if (want_grad) {
-      // recompute p_{s-1} .. p_e of the segment
-      if ((rc = save_or_restore(chk[c], s, false))) return rc;
-      awc::plan_set_step(plan, s);
-      ADJ_TRY(C, cudaMemcpyAsync(seg[0], V.buf[s % 3], fb, cudaMemcpyDeviceToDevice, st));
-      ADJ_TRY(C, cudaMemcpyAsync(seg[1], V.buf[(s + 1) % 3], fb, cudaMemcpyDeviceToDevice, st));
-      awc::plan_keep_fields(plan, (void* const*)(seg.data() + 2), s, e - s);
-      rc = awc_plan_run(plan, e - s, 1, nullptr);
-      awc::plan_keep_fields(plan, nullptr, 0, 0);
-      if (rc) return rc;
-    }
+    const int b = want_grad ? (int)(c % nset) : 0;
+    if (want_grad) ADJ_TRY(C, cudaStreamWaitEvent(bs, ev_rec, 0));
     for (int64_t t = e - 1; t >= s; --t) {
       // λ_{t+1} overwrites λ_{t+3}, which the step kernels read only at the
       // node they write
@@ -1053,40 +1091,44 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
           A.mu_out[a][sd] = mu[a][sd][par ^ 1];
         }
       if (!RG.node.empty())
-        awc::adj_residuals<T><<<(unsigned)((RG.node.size() + 127) / 128), 128, 0, st>>>(
+        awc::adj_residuals<T><<<(unsigned)((RG.node.size() + 127) / 128), 128, 0, bs>>>(
             A.lam, rnode_d, roff_d, rids_d, (int32_t)RG.node.size(), res_d + t * nrec);
-      A.pm1 = want_grad ? seg[t - s] : nullptr;
-      A.p0 = want_grad ? seg[t - s + 1] : nullptr;
-      A.pp1 = want_grad ? seg[t - s + 2] : nullptr;
+      A.pm1 = want_grad ? seg[b][t - s] : nullptr;
+      A.p0 = want_grad ? seg[b][t - s + 1] : nullptr;
+      A.pp1 = want_grad ? seg[b][t - s + 2] : nullptr;
       A.grad = grad;
-      // the shell kernel on the second stream, the core kernel on the main one
       const bool fork = has_core && shell_blocks > 0;
       if (fork) {
-        ADJ_TRY(C, cudaEventRecord(C->ev_fork, st));
-        ADJ_TRY(C, cudaStreamWaitEvent(C->stream2, C->ev_fork, 0));
+        ADJ_TRY(C, cudaEventRecord(ev_fork, bs));
+        ADJ_TRY(C, cudaStreamWaitEvent(bs2, ev_fork, 0));
       }
       if (shell_blocks > 0)
-        launch_shell(A, p->ndim, want_grad, i64, shell_blocks, fork ? C->stream2 : st);
+        launch_shell(A, p->ndim, want_grad, i64, shell_blocks, fork ? bs2 : bs);
       if (has_core && use_tma) {
         awc::adj_core_tma<T, ADJ_TY, ADJ_STAGES>
-            <<<tma_grid, dim3(32, ADJ_TY), adj_core_smem<T>(), st>>>(
-                map_lam[i2], map_f, map_seg[t - s + 1], map_lam3[i3], map_grad, A);
+            <<<tma_grid, dim3(32, ADJ_TY), adj_core_smem<T>(), bs>>>(
+                map_lam[i2], map_f, map_seg[b][t - s + 1], map_lam3[i3], map_grad, A);
       } else if (has_core) {
-        launch_core(A, p->ndim, want_grad, i64, core_grid, st);
+        launch_core(A, p->ndim, want_grad, i64, core_grid, bs);
       }
       if (fork) {
-        ADJ_TRY(C, cudaEventRecord(C->ev_join, C->stream2));
-        ADJ_TRY(C, cudaStreamWaitEvent(st, C->ev_join, 0));
+        ADJ_TRY(C, cudaEventRecord(ev_join, bs2));
+        ADJ_TRY(C, cudaStreamWaitEvent(bs, ev_join, 0));
       }
       if (nsrc > 0)
-        awc::adj_sources<T><<<1, 32, 0, st>>>(A.lam, A.F, snode_d, sband_d, (int32_t)nsrc,
+        awc::adj_sources<T><<<1, 32, 0, bs>>>(A.lam, A.F, snode_d, sband_d, (int32_t)nsrc,
                                               stf_d + t * nsrc, grad,
                                               sout_d ? sout_d + t * nsrc : nullptr);
       ADJ_TRY(C, cudaGetLastError());
       std::swap(i2, i3);  // λ_{t+1} is the next step's λ_{t+2}
       par ^= 1;
     }
+    ADJ_TRY(C, cudaEventRecord(ev_free[b], bs));
+    if (want_grad && c > 0 && (rc = recompute(c - 1))) return rc;
   }
+  // the outputs follow the backward steps
+  ADJ_TRY(C, cudaEventRecord(ev_join, bs));
+  ADJ_TRY(C, cudaStreamWaitEvent(st, ev_join, 0));
   // outputs
   if (want_grad) {
     double* dense;

@@ -1659,6 +1659,13 @@ void awc_destroy(awc_ctx* ctx) {
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  for (cudaStream_t& a : ctx->adj_stream)
+    if (a) {
+      cudaStreamSynchronize(a);
+      cudaStreamDestroy(a);
+    }
+  for (cudaEvent_t& e : ctx->adj_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->host_stage) cudaFreeHost(ctx->host_stage);

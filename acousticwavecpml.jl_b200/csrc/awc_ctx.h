@@ -29,6 +29,11 @@ struct awc_ctx {
   awc_plan* adj_plan = nullptr;
   void* adj_mem = nullptr;
   std::function<void()> adj_release;
+  // the adjoint's backward steps run on their own two streams, so that a
+  // segment's recompute (on `stream`) overlaps the previous segment's
+  // backward steps; events: fork, join, recomputed, segment set 0/1 free
+  cudaStream_t adj_stream[2] = {nullptr, nullptr};
+  cudaEvent_t adj_ev[5] = {};
   // pinned host staging buffer for large pageable copies (grown on demand)
   void* host_stage = nullptr;
   size_t host_stage_bytes = 0;
