@@ -1982,10 +1982,11 @@ namespace {
 int time_shape(awc_plan* P, int64_t n, float* per) {
   int rc;
   *per = 1e30f;
+  // replays of a captured run, as the solves run (the capture is not timed)
   for (int rep = 0; rep < 2; ++rep) {
     if ((rc = awc_plan_reset(P)) || (rc = awc_plan_run(P, 2, 0, nullptr))) return rc;  // warm-up
     float ms = 0.f;
-    if ((rc = awc_plan_run(P, n, 0, &ms))) return rc;
+    if ((rc = awc_plan_run(P, n, 1, &ms))) return rc;
     *per = std::min(*per, ms / (float)n);
   }
   return AWC_OK;
@@ -2032,7 +2033,7 @@ int awc_plan_autotune(awc_plan* P, int64_t steps, float* best_ms_per_step) {
   // phase 2: z planes per block of the band kernel
   if (P->nbox > 0) {
     int32_t wz = P->szc;
-    for (int32_t zc : {4, 6, 8, 10, 12, 16, 20, 32}) {
+    for (int32_t zc : {4, 6, 8, 10, 12, 16, 20, 24, 28, 30, 32, 36, 40}) {
       P->szc = zc;
       box_blocks(P);
       float per = 0.f;
@@ -2044,6 +2045,20 @@ int awc_plan_autotune(awc_plan* P, int64_t steps, float* best_ms_per_step) {
     }
     P->szc = wz;
     box_blocks(P);
+    // the core z chunk again, next to its winner, with the band's chunk set
+    const int32_t zc0 = P->zchunk;
+    int32_t wc = zc0;
+    for (int32_t d : {-2, -1, 1, 2}) {
+      if (zc0 + d < 1) continue;
+      P->zchunk = zc0 + d;
+      float per = 0.f;
+      if ((rc = time_shape(P, n, &per))) return rc;
+      if (per < best) {
+        best = per;
+        wc = zc0 + d;
+      }
+    }
+    P->zchunk = wc;
   }
   // phase 3: two-step passes, z chunks per column tile
   if (tb_eligible(P)) {

@@ -471,7 +471,7 @@ def main():
     if args.launch:
         plan.set_launch(*[int(x) for x in args.launch.split(",")])
     else:
-        plan.autotune(40)  # launch shape picked on this data, before any timing
+        plan.autotune(120)  # launch shape picked on this data, before any timing
     if args.blocking:
         plan.set_blocking(*[int(x) for x in args.blocking.split(",")])
     launch = plan.get_launch()
