@@ -533,6 +533,46 @@ __global__ void adj_residuals(T* __restrict__ lam3, const int64_t* __restrict__ 
   lam3[node[n]] = v;
 }
 
+// The residual rows [nt][nrec] in the working precision from a column-major
+// (nt x nrec) double array d: rows[t][r] = traces[t][r] - d[t + nt r] when
+// traces is given (d = observed data), else d itself (the adjoint traces).
+// 32 x 32 tiles through shared memory (coalesced on both sides); with traces,
+// each block also writes its sum of res² / 2 to part[block].
+template <typename T>
+__global__ void __launch_bounds__(256) adj_residual_rows(const T* __restrict__ traces,
+                                                         const double* __restrict__ d, int64_t nt,
+                                                         int64_t nrec, T* __restrict__ rows,
+                                                         double* __restrict__ part) {
+  __shared__ double tile[32][33];
+  __shared__ double wsum[8];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int64_t r0 = (int64_t)blockIdx.x * 32, t0 = (int64_t)blockIdx.y * 32;
+  for (int q = ty; q < 32; q += 8) {
+    const int64_t t = t0 + tx, r = r0 + q;
+    tile[q][tx] = (t < nt && r < nrec) ? d[t + nt * r] : 0.0;
+  }
+  __syncthreads();
+  double acc = 0.0;
+  for (int q = ty; q < 32; q += 8) {
+    const int64_t t = t0 + q, r = r0 + tx;
+    if (t < nt && r < nrec) {
+      double v = tile[tx][q];
+      if (traces) v = (double)traces[t * nrec + r] - v;
+      rows[t * nrec + r] = (T)v;
+      acc += 0.5 * v * v;
+    }
+  }
+  if (!part) return;
+  for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+  if (tx == 0) wsum[ty] = acc;
+  __syncthreads();
+  if (tx == 0 && ty == 0) {
+    double b = 0.0;
+    for (int w = 0; w < 8; ++w) b += wsum[w];
+    part[blockIdx.x + (int64_t)gridDim.x * blockIdx.y] = b;
+  }
+}
+
 // Per source (one thread, serial over sources for a fixed summation order):
 // the adjoint of the injected value, λ_{t+1} at the source node, and the
 // removal of the source term from the gradient bracket.
@@ -850,9 +890,15 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
     ADJ_TRY(C, cudaMemsetAsync(grad, 0, NP * sizeof(double), st));
   }
   // source rows [nt][nsrc] in T (the residual rows follow the forward run)
-  std::vector<T> rows(std::max<int64_t>(nt * nrec, 1));
+  // residual rows [nt][nrec] (device) from column-major doubles uploaded to colm_d
   T* res_d;
-  ADJ_TRY(C, mem.get(&res_d, rows.size() * sizeof(T)));
+  ADJ_TRY(C, mem.get(&res_d, std::max<int64_t>(nt * nrec, 1) * sizeof(T)));
+  double* colm_d;
+  ADJ_TRY(C, mem.get(&colm_d, std::max<int64_t>(nt * nrec, 1) * sizeof(double)));
+  const dim3 rgrid((unsigned)std::max<int64_t>(1, (nrec + 31) / 32),
+                   (unsigned)std::max<int64_t>(1, (nt + 31) / 32));
+  double* part_d;
+  ADJ_TRY(C, mem.get(&part_d, (size_t)rgrid.x * rgrid.y * sizeof(double)));
   std::vector<T> srows(std::max<int64_t>(nt * nsrc, 1), T(0));
   if (dt2srctf)
     for (int64_t s = 0; s < nsrc; ++s)
@@ -1022,7 +1068,6 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
     return AWC_OK;
   };
   int rc;
-  std::vector<double> res_h;
   if (want_grad) {
     // forward run with checkpoints, then the traces, misfit and residuals
     if ((rc = awc_plan_reset(plan))) return rc;
@@ -1031,20 +1076,27 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
       if ((rc = save_or_restore(chk[c], s, true))) return rc;
       if ((rc = awc_plan_run(plan, std::min(kchk, nt - s), 1, nullptr))) return rc;
     }
-    res_h.assign(std::max<int64_t>(nt * nrec, 1), 0.0);
-    if (nt * nrec > 0 && (rc = awc_plan_traces(plan, res_h.data()))) return rc;
-    if (traces_out && nt * nrec > 0) std::memcpy(traces_out, res_h.data(), nt * nrec * sizeof(double));
-    double J = 0.0;
-    for (int64_t c = 0; c < nt * nrec; ++c) {
-      res_h[c] -= observed[c];
-      J += 0.5 * res_h[c] * res_h[c];
-    }
-    *misfit = J;
-    residual = res_h.data();
+    if (traces_out && nt * nrec > 0 && (rc = awc_plan_traces(plan, traces_out))) return rc;
   }
-  for (int64_t r = 0; r < nrec; ++r)
-    for (int64_t t = 0; t < nt; ++t) rows[t * nrec + r] = (T)residual[t + nt * r];
-  ADJ_TRY(C, cudaMemcpyAsync(res_d, rows.data(), rows.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+  if (want_grad) *misfit = 0.0;
+  if (nt * nrec > 0) {
+    // residuals (and the misfit's block sums) on the device
+    ADJ_TRY(C, awc::copy_to_device(C, colm_d, want_grad ? observed : residual,
+                                   nt * nrec * sizeof(double), st));
+    awc::adj_residual_rows<T><<<rgrid, dim3(32, 8), 0, st>>>(
+        want_grad ? (const T*)V.traces : nullptr, colm_d, nt, nrec, res_d,
+        want_grad ? part_d : nullptr);
+    ADJ_TRY(C, cudaGetLastError());
+    if (want_grad) {
+      std::vector<double> part((size_t)rgrid.x * rgrid.y);
+      ADJ_TRY(C, cudaMemcpyAsync(part.data(), part_d, part.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st));
+      ADJ_TRY(C, cudaStreamSynchronize(st));
+      double J = 0.0;
+      for (double v : part) J += v;  // fixed order
+      *misfit = J;
+    }
+  }
   // backward: the steps run on the adjoint's two streams (core kernel on the
   // first, shell kernel on the second); segment c - 1 is recomputed on the
   // plan's stream into the other field set meanwhile
