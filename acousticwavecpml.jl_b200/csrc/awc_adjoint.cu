@@ -1072,9 +1072,19 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
     // forward run with checkpoints, then the traces, misfit and residuals
     if ((rc = awc_plan_reset(plan))) return rc;
     for (int64_t c = 0; c < nseg; ++c) {
-      const int64_t s = c * kchk;
+      const int64_t s = c * kchk, e = std::min(s + kchk, nt);
       if ((rc = save_or_restore(chk[c], s, true))) return rc;
-      if ((rc = awc_plan_run(plan, std::min(kchk, nt - s), 1, nullptr))) return rc;
+      if (c == nseg - 1) {
+        // the last segment's fields are kept as they are computed, so the
+        // backward pass starts without a recompute
+        std::vector<T*>& f = seg[c % nset];
+        ADJ_TRY(C, cudaMemcpyAsync(f[0], V.buf[s % 3], fb, cudaMemcpyDeviceToDevice, st));
+        ADJ_TRY(C, cudaMemcpyAsync(f[1], V.buf[(s + 1) % 3], fb, cudaMemcpyDeviceToDevice, st));
+        awc::plan_keep_fields(plan, (void* const*)(f.data() + 2), s, e - s);
+      }
+      rc = awc_plan_run(plan, e - s, 1, nullptr);
+      awc::plan_keep_fields(plan, nullptr, 0, 0);
+      if (rc) return rc;
     }
     if (traces_out && nt * nrec > 0 && (rc = awc_plan_traces(plan, traces_out))) return rc;
   }
@@ -1125,7 +1135,6 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
   };
   int i2 = 0, i3 = 1;  // lam[i2] = λ_{t+2}, lam[i3] = λ_{t+3}
   int par = 0;         // nu[..][par] holds ν_{t+2}
-  if (want_grad && (rc = recompute(nseg - 1))) return rc;
   for (int64_t c = (want_grad ? nseg : 1) - 1; c >= 0; --c) {
     const int64_t s = want_grad ? c * kchk : 0, e = want_grad ? std::min(s + kchk, nt) : nt;
     const int b = want_grad ? (int)(c % nset) : 0;
