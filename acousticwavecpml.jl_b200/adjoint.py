@@ -111,12 +111,17 @@ def sharded_gradient(shots, shot_gradient, shape, group=None):
     on = dist.is_available() and dist.is_initialized()
     rank = dist.get_rank(group) if on else 0
     world = dist.get_world_size(group) if on else 1
-    total = np.zeros(shape)
+    total = np.zeros(shape, order="F")  # the layout misfit_gradient returns
+    tt = torch.from_numpy(total.reshape(-1, order="F"))  # a view: torch adds on all cores
     J = 0.0
     for shot in shots[rank::world]:
         j, g = shot_gradient(shot)
         J += j
-        total += g
+        g = np.asarray(g, dtype=np.float64)
+        if g.shape != total.shape:
+            raise ValueError(f"shot_gradient returned shape {g.shape}, expected {total.shape}")
+        gv = g if g.flags.f_contiguous else np.asfortranarray(g)
+        tt.add_(torch.from_numpy(gv.reshape(-1, order="F")))
     if on:
         buf = torch.from_numpy(np.concatenate([total.ravel(order="F"), [J]]))
         dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"

@@ -366,59 +366,72 @@ def batch_profile_run(args, local):
 
 
 def gradient_leg(pkg, ctx, rank, world, timed_host):
-    """3D gradient, FP32 with an FP64 check: one shot of the 16-shot
-    gradient workload per rank (shot = rank), dJ/d(c²) at the initial model
-    against the true model's traces of the same precision, through
-    awc_misfit_gradient (host
-    buffers, checkpoint every 50 steps, nt = 1500); under torchrun the ranks'
-    gradients are then summed with one all-reduce."""
+    """3D gradient, FP32 with an FP64 check: config 4's 16 shots, dJ/d(c²)
+    summed over the shots at the initial model against the true model's
+    traces of the same precision, through awc_misfit_gradient (host buffers,
+    checkpoint every 50 steps, nt = 1500). Rank r takes shots r, r + N, ...;
+    under torchrun the ranks' sums are added with one all-reduce
+    (adjoint.sharded_gradient). The FP64 build checks shot 0."""
     import time
     import torch
     import torch.distributed as dist
     from acousticwavecpml_b200 import adjoint
     from acousticwavecpml_b200 import workloads as W
     w = W.config4()
-    S = pkg.Sources(w["shots"][rank % len(w["shots"])], w["t0s"], [pkg.rickersource1D], w["f0"])
     R = pkg.Receivers(w["rec_pos"])
     kw = dict(w["kwargs"])
-    st = pkg.prepare(w["lengths"], None, w["true"], S, R, precision="f32", **kw)
-    p = st["problem"]
-    obs = np.zeros((p.nt, p.nrec), order="F")
-    ctx.forward(p, st["vel"], st["coeffs"], st["possrcs"], st["dt2srctf"], st["posrecs"], obs)
+    nshot = len(w["shots"])
+
+    def setups(shot, precision):
+        S = pkg.Sources(w["shots"][shot], w["t0s"], [pkg.rickersource1D], w["f0"])
+        st = pkg.prepare(w["lengths"], None, w["true"], S, R, precision=precision, **kw)
+        si = pkg.prepare(w["lengths"], None, w["init"], S, R, precision=precision, **kw)
+        si["coeffs"] = st["coeffs"]  # the CPML profile of the true model's vmax
+        p = st["problem"]
+        obs = np.zeros((p.nt, p.nrec), order="F")
+        ctx.forward(p, st["vel"], st["coeffs"], st["possrcs"], st["dt2srctf"], st["posrecs"], obs)
+        return st, si, obs
+
+    # observed data of every shot of this rank (not timed)
+    mine = list(range(rank, nshot, world))
+    data = {k: setups(k, "f32") for k in (mine or [0])}
+    st0, si0, obs0 = data[(mine or [0])[0]]
+    p = st0["problem"]
     t0 = time.perf_counter()
-    ctx.forward(p, st["vel"], st["coeffs"], st["possrcs"], st["dt2srctf"], st["posrecs"], obs)
+    ctx.forward(p, si0["vel"], si0["coeffs"], si0["possrcs"], si0["dt2srctf"], si0["posrecs"],
+                np.zeros((p.nt, p.nrec), order="F"))
     t_fwd = time.perf_counter() - t0
-    si = pkg.prepare(w["lengths"], None, w["init"], S, R, precision="f32", **kw)
-    si["coeffs"] = st["coeffs"]  # the CPML profile of the true model's vmax
-    adjoint.misfit_gradient(si, obs, w["checkpoint_every"], ctx)  # warm-up
-    t_grad = timed_host(lambda: adjoint.misfit_gradient(si, obs, w["checkpoint_every"], ctx))
-    J32, g32, _ = adjoint.misfit_gradient(si, obs, w["checkpoint_every"], ctx)
-    # the FP64 build on FP64 data of the true model
-    s64t = pkg.prepare(w["lengths"], None, w["true"], S, R, precision="f64", **kw)
-    obs64 = np.zeros((p.nt, p.nrec), order="F")
-    ctx.forward(s64t["problem"], s64t["vel"], s64t["coeffs"], s64t["possrcs"], s64t["dt2srctf"],
-                s64t["posrecs"], obs64)
-    s64 = pkg.prepare(w["lengths"], None, w["init"], S, R, precision="f64", **kw)
-    s64["coeffs"] = st["coeffs"]
-    J64, g64, _ = adjoint.misfit_gradient(s64, obs64, w["checkpoint_every"], ctx)
+    adjoint.misfit_gradient(si0, obs0, w["checkpoint_every"], ctx)  # warm-up
+
+    def one_shot(k):
+        _, si, obs = data[k]
+        J, g, _ = adjoint.misfit_gradient(si, obs, w["checkpoint_every"], ctx)
+        return J, g
+
+    out = {}
+    t_grad = timed_host(lambda: out.update(
+        r=adjoint.sharded_gradient(list(range(nshot)), one_shot, w["init"].shape)))
+    J32_all, g32_all = out["r"]
+    # FP64 check on shot 0 (rank 0's first shot), against its own FP64 data
+    J32, g32 = one_shot((mine or [0])[0])
     t_ar = 0.0
-    if world > 1:
-        buf = torch.from_numpy(np.ascontiguousarray(g32.ravel(order="F"))).cuda()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        dist.all_reduce(buf)
-        torch.cuda.synchronize()
-        t_ar = time.perf_counter() - t0
-    return {"workload": w["name"], "dtype": "f32", "shots_per_rank": 1,
-            "value": world / t_grad, "unit": "shot gradients/s",
-            "s_per_gradient": t_grad, "s_per_forward": t_fwd,
-            "gradient_over_forward": t_grad / t_fwd, "checkpoint_every": w["checkpoint_every"],
-            "nt": p.nt, "grid": [p.nx, p.ny, p.nz],
-            "fp32_vs_fp64_gradient_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
-            "fp32_vs_fp64_misfit_rel": abs(J32 - J64) / J64,
-            "allreduce_s": t_ar,
-            "timing": "host wall clock of the C-ABI call (uploads, checkpointed forward, "
-                      "recompute, adjoint, download), max over ranks"}
+    res = {}
+    if rank == 0:
+        _, s64, obs64 = setups(0, "f64")
+        s64["coeffs"] = si0["coeffs"]
+        J64, g64, _ = adjoint.misfit_gradient(s64, obs64, w["checkpoint_every"], ctx)
+        res = {"fp32_vs_fp64_gradient_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+               "fp32_vs_fp64_misfit_rel": abs(J32 - J64) / J64}
+    return {"workload": w["name"], "dtype": "f32", "shots": nshot, "shots_per_rank": len(mine),
+            "value": nshot / t_grad, "unit": "shot gradients/s",
+            "s_for_all_shots": t_grad, "s_per_gradient": t_grad * world / nshot,
+            "s_per_forward": t_fwd, "gradient_over_forward": t_grad * world / nshot / t_fwd,
+            "misfit_all_shots": float(J32_all), "checkpoint_every": w["checkpoint_every"],
+            "nt": p.nt, "grid": [p.nx, p.ny, p.nz], **res,
+            "check_shot": 0,
+            "timing": "host wall clock of the per-shot C-ABI calls (uploads, checkpointed "
+                      "forward, recompute, adjoint, download) and the summation (one all-reduce "
+                      "under torchrun), max over ranks"}
 
 
 def main():
