@@ -78,6 +78,17 @@ def measured_peak():
         return 6650.0, "fallback 6.65 TB/s"
 
 
+def ncu_value(kernel_tag, key):
+    """A `key: value` figure from the committed ncu summary of a kernel."""
+    path = os.path.join(ROOT, "profiles", f"ncu_{kernel_tag}.md")
+    try:
+        txt = open(path).read()
+    except OSError:
+        return None
+    m = re.search(re.escape(key) + r":\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
 def ncu_traffic(kernel_tag):
     """Per-launch DRAM bytes of the step kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", f"ncu_{kernel_tag}.md")
@@ -279,6 +290,7 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak, keep=None):
     b.close()
     achieved = words * 4 / t_ts / 1e9
     traffic = ncu_traffic("step2d_batch_tma_96shots") if world == 1 else None
+    l2_bytes = ncu_value("step2d_batch_tma_96shots", "l2_bytes_per_launch") if world == 1 else None
     dram = None
     if traffic:
         dram = {"traffic_bytes_per_step": traffic, "achieved": traffic / t_ts / 1e9,
@@ -296,6 +308,10 @@ def batch_leg(pkg, ctx, args, rank, world, timed, peak, keep=None):
                                        "persistent batched-step launch; A_eff summed over "
                                        "shots, FP32 words"},
             "dram_roofline": dram,
+            "l2": ({"traffic_bytes_per_step": l2_bytes, "achieved_gbs": l2_bytes / t_ts / 1e9,
+                    "note": "ncu lts__t_bytes of one step (profiles/) over the measured step "
+                            "time; no measured L2 peak on this pool, so no fraction"}
+                   if l2_bytes else None),
             "launch": {"tile": [64 if ty <= 16 else 32, ty], "blocks_per_sm": bps,
                        "kernel": "step2d_batch_tma (TMA stages, producer warp)" if ty <= 16
                                  else "step2d_batch (register strips)"},
