@@ -266,9 +266,16 @@ __device__ __forceinline__ void adj_shell_node(const AdjStep<T>& A, int i, int j
 // the block's box kind selects the body.
 template <typename T, typename I, int ND, bool GRAD>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) adj_shell(const __grid_constant__ AdjStep<T> A) {
-  int b = 0;
+  // the box of this block: box_blk rises strictly, so a binary search
   const int blk = blockIdx.x;
-  while (b + 1 < A.nbox && blk >= A.box_blk[b + 1]) ++b;
+  int b = 0, hi = A.nbox - 1;
+  while (b < hi) {
+    const int mid = (b + hi + 1) >> 1;
+    if (A.box_blk[mid] <= blk)
+      b = mid;
+    else
+      hi = mid - 1;
+  }
   const Box& B = A.box[b];
   const int W = B.x1 - B.x0 + 1, ncol = W * (B.y1 - B.y0 + 1);
   const int ncb = (ncol + 255) / 256;
