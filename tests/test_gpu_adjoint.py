@@ -104,6 +104,58 @@ def test_gradient_vs_oracle_fd(pkg, oracle, ctx, dim):
         assert abs(grad[cell] - fd) <= 1e-6 * max(abs(fd), 1e-3 * np.abs(grad).max())
 
 
+def _small(dim, n, halo, freetop):
+    """A grid too small for a band-free core (or just large enough)."""
+    d = 10.0
+    rng = np.random.default_rng(sum(n) + halo)
+    shape = n[:dim]
+    vel = 2000.0 + 100.0 * rng.random(shape)
+    L = tuple((m - 1) * d for m in shape)
+    c = [(m // 2) * d for m in shape]
+    srcs = [c, [((shape[0] // 2) + 1) * d] + [2 * d] * (dim - 1)]
+    recs = [[(i - 1) * d] + [3 * d] * (dim - 1) for i in (2, shape[0] // 2, shape[0] - 1)]
+    return L, vel, srcs, recs, dict(halo=halo, rcoef=1e-4, freetop=freetop)
+
+
+@pytest.mark.parametrize("dim,n,halo,freetop", [
+    (3, (12, 13, 12), 4, False),   # the near-band zones meet: one generic shell box
+    (3, (16, 15, 17), 4, True),    # a core of a few nodes
+    (2, (12, 12, 1), 4, False),
+    (3, (14, 12, 13), 0, False),   # no CPML: everything is core
+])
+def test_small_grids_dot_product_and_fd(pkg, oracle, ctx, dim, n, halo, freetop):
+    """The adjoint's region split at its limits: the dot-product test and
+    central differences of the FP64 oracle on a few cells."""
+    from acousticwavecpml_b200 import adjoint
+    L, vel, srcs, recs, kw = _small(dim, n, halo, freetop)
+    s = setup(pkg, L, vel, srcs, recs, kw, lt=0.08)
+    p = s["problem"]
+    rng = np.random.default_rng(5)
+    sa = rng.standard_normal((p.nt, p.nsrc))
+    r = rng.standard_normal((p.nt, p.nrec))
+    lhs = float(np.sum(traces_of(ctx, dict(s, dt2srctf=np.asfortranarray(sa))) * r))
+    rhs = float(np.sum(sa * adjoint.adjoint_sources(s, r, ctx)))
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), abs(rhs))
+    obs = traces_of(ctx, dict(s, vel=np.asfortranarray(np.full_like(vel, vel.mean()))))
+    J, grad, _ = adjoint.misfit_gradient(s, obs, checkpoint_every=9, ctx=ctx)
+
+    def oracle_J(v):
+        so = oracle.setup(L, None, v, srcs, [0.05] * len(srcs), 12.0, recs, check_ppw=False,
+                          dt=s["dt"], nt=p.nt, **kw)
+        so["coeffs"] = s["coeffs"]
+        _, tr = oracle.forward(so)
+        return 0.5 * np.sum((tr - obs) ** 2)
+
+    c2 = vel ** 2
+    for cell in _fd_cells(rng, vel, halo, 6):
+        eps = 1e-4 * c2[cell]
+        vp, vm = vel.copy(), vel.copy()
+        vp[cell] = np.sqrt(c2[cell] + eps)
+        vm[cell] = np.sqrt(c2[cell] - eps)
+        fd = (oracle_J(vp) - oracle_J(vm)) / (2 * eps)
+        assert abs(grad[cell] - fd) <= 1e-6 * max(abs(fd), 1e-3 * np.abs(grad).max()), cell
+
+
 def test_gradient_with_rim_source_vs_oracle_fd(pkg, oracle, ctx):
     """A source on the Dirichlet rim (the free top) feeds the rim value of
     every pressure field, which the Laplacian of the interior nodes below it
