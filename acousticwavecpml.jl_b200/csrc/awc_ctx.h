@@ -22,7 +22,7 @@ struct awc_ctx {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   float last_run_ms = 0.f;
-  int64_t autotune_steps = 10;   // per candidate, for new 3D plans of awc_forward
+  int64_t autotune_steps = 40;   // per candidate, for new 3D plans of awc_forward
   std::vector<awc_plan*> cache;  // plans reused by awc_forward, most recent last
   // the adjoint entry points keep their plan and working memory between
   // calls of one shape (released by awc_destroy or a call of another shape)

@@ -103,7 +103,7 @@ float awc_last_run_ms(const awc_ctx* ctx);
 void* awc_ctx_stream(const awc_ctx* ctx);
 /* Steps per candidate with which awc_forward autotunes the launch shape of
  * each new 3D problem shape (nt >= 100) before its first solve; 0 disables
- * it. Default 10. The choice is cached with the plan. */
+ * it. Default 40. The choice is cached with the plan. */
 int awc_ctx_set_autotune(awc_ctx* ctx, int64_t steps);
 
 /* The forward solve (the time loop of acoustic_3D_xPU.jl:392-409 and the
