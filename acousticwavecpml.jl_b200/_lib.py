@@ -122,6 +122,8 @@ SIGNATURES = {
     "awc_plan_set_wait": (ctypes.c_int, [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
     "awc_misfit_gradient": (ctypes.c_int, [_vp, _PP, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int32,
                                            _vp, _vp, _vp]),
+    "awc_misfit_gradient_shots": (ctypes.c_int, [_vp, _PP, ctypes.c_int32, _vp, _vp, _vp, _vp,
+                                                 _vp, _vp, ctypes.c_int32, _vp, _vp]),
     "awc_adjoint_sources": (ctypes.c_int, [_vp, _PP, _vp, _vp, _vp, _vp, _vp, _vp]),
     "awc_learned_weights_len": (ctypes.c_int, [ctypes.c_int32]),
     "awc_forward_learned": (ctypes.c_int, [_vp, _PP, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -6,6 +6,8 @@ The reference has no gradient. These functions take the same shot set-up as
 solve2D/solve3D (a prepare() dict) and add:
   * misfit_gradient: J = 1/2 Σ (traces - observed)² and dJ/d(c²), with the
     forward state checkpointed every k steps and recomputed per segment;
+  * misfit_gradient_shots: the same summed over the shots of one model in
+    one call (the model uploaded once, the gradients summed on the device);
   * adjoint_sources: the transpose of the map from injected source values to
     traces, for dot-product tests;
   * C2Misfit: a torch.autograd.Function over c², so the solver takes part in
@@ -41,6 +43,52 @@ def misfit_gradient(s, observed, checkpoint_every=50, ctx=None):
                                          int(checkpoint_every), ctypes.byref(J), _ptr(grad),
                                          _ptr(traces)), ctx.handle)
     return float(J.value), grad, traces
+
+
+def misfit_gradient_shots(setups, observed, checkpoint_every=50, ctx=None):
+    """(Σ J, Σ dJ/dc²) over shots of one model, equal to summing
+    misfit_gradient over the shots in order. setups[s] is shot s's prepare()
+    dict: all share the problem, vel, coeffs and receivers, and only their
+    sources differ. observed: one (nt x nrec) array per shot, or all of them
+    as one (nt x nrec x nshot) array (used without a copy when it is a
+    Fortran-ordered float64 array)."""
+    ctx = ctx or default_context()
+    if not setups:
+        raise ValueError("no shots")
+    s0 = setups[0]
+    p = s0["problem"]
+
+    def same(a, b):
+        return a is b or np.array_equal(a, b)
+
+    for s in setups[1:]:
+        q = s["problem"]
+        if any(getattr(q, f) != getattr(p, f) for f, _ in type(p)._fields_):
+            raise ValueError("every shot needs the same problem (grid, nt, nsrc, nrec)")
+        if not (same(s["vel"], s0["vel"]) and same(s["coeffs"], s0["coeffs"])
+                and same(s["posrecs"], s0["posrecs"])):
+            raise ValueError("every shot needs the same vel, coeffs and receivers")
+    if isinstance(observed, np.ndarray) and observed.ndim == 3:
+        obs = np.asfortranarray(observed, dtype=np.float64)
+    else:
+        if len(observed) != len(setups):
+            raise ValueError("one observed array per shot")
+        obs = np.stack([np.asarray(o, dtype=np.float64) for o in observed], axis=-1)
+        obs = np.asfortranarray(obs)
+    if obs.shape != (p.nt, p.nrec, len(setups)):
+        raise ValueError(f"observed must be (nt, nrec) = ({p.nt}, {p.nrec}) per shot")
+    pos = np.asfortranarray(np.stack([np.asarray(s["possrcs"], dtype=np.int64) for s in setups],
+                                     axis=-1))
+    stf = np.asfortranarray(np.stack([np.asarray(s["dt2srctf"], dtype=np.float64)
+                                      for s in setups], axis=-1))
+    grad = np.zeros(s0["vel"].shape, order="F")
+    J = ctypes.c_double(0.0)
+    check(_lib.lib().awc_misfit_gradient_shots(ctx.handle, ctypes.byref(p), len(setups),
+                                               _ptr(s0["vel"]), _ptr(s0["coeffs"]), _ptr(pos),
+                                               _ptr(stf), _ptr(s0["posrecs"]), _ptr(obs),
+                                               int(checkpoint_every), ctypes.byref(J),
+                                               _ptr(grad)), ctx.handle)
+    return float(J.value), grad
 
 
 def adjoint_sources(s, adjoint_traces, ctx=None):
@@ -99,12 +147,14 @@ except ImportError:  # torch is optional for the C-ABI users of this package
     C2Misfit = None
 
 
-def sharded_gradient(shots, shot_gradient, shape, group=None):
+def sharded_gradient(shots, shot_gradient, shape, group=None, batched=False):
     """Σ over shots of (J, dJ/dc²) when each rank of a torch.distributed group
     takes shots rank, rank + N, ...: every rank calls shot_gradient(shot) ->
     (J, grad ndarray of `shape`) for its share, sums them, and one all-reduce
-    (sum) of [grad, J] gives every rank the total. Without an initialised
-    process group it sums all shots locally."""
+    (sum) of [grad, J] gives every rank the total. With batched=True the rank
+    makes one call, shot_gradient(list of its shots) -> their summed (J, grad)
+    (e.g. misfit_gradient_shots). Without an initialised process group it sums
+    all shots locally."""
     import torch
     import torch.distributed as dist
 
@@ -114,7 +164,9 @@ def sharded_gradient(shots, shot_gradient, shape, group=None):
     total = np.zeros(shape, order="F")  # the layout misfit_gradient returns
     tt = torch.from_numpy(total.reshape(-1, order="F"))  # a view: torch adds on all cores
     J = 0.0
-    for shot in shots[rank::world]:
+    mine = list(shots[rank::world])
+    calls = ([mine] if mine else []) if batched else mine
+    for shot in calls:
         j, g = shot_gradient(shot)
         J += j
         g = np.asarray(g, dtype=np.float64)

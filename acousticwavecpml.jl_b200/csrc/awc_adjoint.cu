@@ -607,6 +607,17 @@ __global__ void scale_unpitch(const double* __restrict__ src, double* __restrict
   }
 }
 
+// dst (dense) += scale * src (pitched), each product rounded before the sum:
+// the same arithmetic as scale_unpitch followed by a host-side sum.
+__global__ void scale_unpitch_add(const double* __restrict__ src, double* __restrict__ dst,
+                                  int64_t n, int64_t nx, int64_t px, double scale) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = c % nx, r = c / nx;
+    dst[c] = __dadd_rn(dst[c], __dmul_rn(scale, src[i + px * r]));
+  }
+}
+
 template <typename T>
 __global__ void to_double(const T* __restrict__ src, double* __restrict__ dst, int64_t n) {
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
@@ -636,11 +647,28 @@ namespace {
 struct DevMem {
   std::vector<std::pair<void*, size_t>> blocks;
   size_t next = 0;
+  void* sum = nullptr;  // the multi-shot gradient sum, outside the per-call blocks
+  size_t sum_bytes = 0;
   void begin() { next = 0; }
   void release() {
     for (auto& b : blocks) cudaFree(b.first);
     blocks.clear();
     next = 0;
+    if (sum) cudaFree(sum);
+    sum = nullptr;
+    sum_bytes = 0;
+  }
+  cudaError_t get_sum(double** out, size_t bytes) {
+    if (sum_bytes != bytes) {
+      if (sum) cudaFree(sum);
+      sum = nullptr;
+      sum_bytes = 0;
+      cudaError_t e = cudaMalloc(&sum, bytes);
+      if (e != cudaSuccess) return e;
+      sum_bytes = bytes;
+    }
+    *out = (double*)sum;
+    return cudaSuccess;
   }
   ~DevMem() { release(); }
   template <typename P>
@@ -865,18 +893,20 @@ int adj_streams(awc_ctx* C, cudaStream_t* a, cudaStream_t* b) {
 }
 
 template <typename T>
-// Gradient mode (grad_out set): the checkpointed forward run gives the
-// traces, the misfit against `observed` and the residuals. Transpose mode
-// (src_out set): `residual` are the adjoint traces.
+// Gradient mode (grad_out or grad_sum set): the checkpointed forward run
+// gives the traces, the misfit against `observed` and the residuals; the
+// gradient goes to the host (grad_out) or is added to a dense device sum
+// (grad_sum). Transpose mode (src_out set): `residual` are the adjoint traces.
 int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double* coeffs,
                  const int64_t* possrcs, const double* dt2srctf, const int64_t* posrecs,
                  const double* residual, const double* observed, double* misfit,
-                 double* traces_out, int64_t kchk, double* grad_out, double* src_out) {
+                 double* traces_out, int64_t kchk, double* grad_out, double* src_out,
+                 double* grad_sum = nullptr) {
   const awc::PlanView V = awc::plan_view(plan);
   cudaStream_t st = V.stream;
   const int64_t nt = p->nt, nsrc = p->nsrc, nrec = p->nrec, h = p->halo;
   const int64_t NP = V.NP, fb = NP * (int64_t)sizeof(T);
-  const bool want_grad = grad_out != nullptr;
+  const bool want_grad = grad_out != nullptr || grad_sum != nullptr;
   DevMem& mem = ctx_mem(C);
   // adjoint fields
   T *lam[2], *mu[3][2][2] = {}, *nu[3][2][2] = {};
@@ -1199,13 +1229,19 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
   ADJ_TRY(C, cudaStreamWaitEvent(st, ev_join, 0));
   // outputs
   if (want_grad) {
-    double* dense;
     const int64_t N = p->nx * p->ny * V.nz;
-    ADJ_TRY(C, mem.get(&dense, N * sizeof(double)));
     const int blocks = (int)std::min<int64_t>((N + 255) / 256, (int64_t)C->num_sms * 16);
-    awc::scale_unpitch<<<blocks, 256, 0, st>>>(grad, dense, N, p->nx, V.px, p->dt * p->dt);
-    ADJ_TRY(C, cudaGetLastError());
-    ADJ_TRY(C, awc::copy_to_host(C, grad_out, dense, N * sizeof(double), st));
+    if (grad_sum) {
+      awc::scale_unpitch_add<<<blocks, 256, 0, st>>>(grad, grad_sum, N, p->nx, V.px,
+                                                     p->dt * p->dt);
+      ADJ_TRY(C, cudaGetLastError());
+    } else {
+      double* dense;
+      ADJ_TRY(C, mem.get(&dense, N * sizeof(double)));
+      awc::scale_unpitch<<<blocks, 256, 0, st>>>(grad, dense, N, p->nx, V.px, p->dt * p->dt);
+      ADJ_TRY(C, cudaGetLastError());
+      ADJ_TRY(C, awc::copy_to_host(C, grad_out, dense, N * sizeof(double), st));
+    }
   }
   if (src_out && nsrc > 0) {
     double* sd;
@@ -1265,6 +1301,53 @@ int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
            : adjoint_impl<float>(ctx, plan, p, coeffs, possrcs, dt2srctf, posrecs, nullptr,
                                  observed, misfit, traces, checkpoint_every, grad_c2, nullptr);
   return rc;
+}
+
+int awc_misfit_gradient_shots(awc_ctx* ctx, const awc_problem* p, int32_t nshot,
+                              const double* vel, const double* coeffs, const int64_t* possrcs,
+                              const double* dt2srctf, const int64_t* posrecs,
+                              const double* observed, int32_t checkpoint_every, double* misfit,
+                              double* grad_c2) {
+  if (!ctx) return awc::fail(nullptr, AWC_ERR_INVALID, "ctx is NULL");
+  int rc;
+  if ((rc = check_adjoint_problem(ctx, p))) return rc;
+  if (nshot < 1) return awc::fail(ctx, AWC_ERR_INVALID, "nshot must be >= 1");
+  if (!observed || !grad_c2 || !misfit)
+    return awc::fail(ctx, AWC_ERR_INVALID, "observed/grad_c2/misfit is NULL");
+  if (p->nsrc > 0 && (!possrcs || (p->nt > 0 && !dt2srctf)))
+    return awc::fail(ctx, AWC_ERR_INVALID, "possrcs/dt2srctf is NULL");
+  if (checkpoint_every < 1) return awc::fail(ctx, AWC_ERR_INVALID, "checkpoint_every must be >= 1");
+  // per-shot strides of the stacked inputs
+  const int64_t s_pos = p->nsrc * p->ndim, s_stf = p->nt * p->nsrc, s_obs = p->nt * p->nrec;
+  auto pos_of = [&](int32_t s) { return p->nsrc > 0 ? possrcs + s * s_pos : possrcs; };
+  auto stf_of = [&](int32_t s) { return dt2srctf ? dt2srctf + s * s_stf : dt2srctf; };
+  // the first shot uploads the model; the others replace only the sources
+  if ((rc = awc::plan_for(ctx, &ctx->adj_plan, p, vel, coeffs, pos_of(0), stf_of(0), posrecs,
+                          true)))
+    return rc;
+  awc_plan* plan = ctx->adj_plan;
+  const cudaStream_t st = awc::plan_view(plan).stream;
+  const int64_t N = p->nx * p->ny * (p->ndim == 3 ? p->nz : 1);
+  double* sum;
+  ADJ_TRY(ctx, ctx_mem(ctx).get_sum(&sum, N * sizeof(double)));
+  ADJ_TRY(ctx, cudaMemsetAsync(sum, 0, N * sizeof(double), st));
+  double J = 0.0;
+  for (int32_t s = 0; s < nshot; ++s) {
+    if (s > 0 && (rc = awc::plan_shot(ctx, plan, pos_of(s), stf_of(s), posrecs))) return rc;
+    double Js = 0.0;
+    rc = p->precision == AWC_F64
+             ? adjoint_impl<double>(ctx, plan, p, coeffs, pos_of(s), stf_of(s), posrecs, nullptr,
+                                    observed + s * s_obs, &Js, nullptr, checkpoint_every,
+                                    nullptr, nullptr, sum)
+             : adjoint_impl<float>(ctx, plan, p, coeffs, pos_of(s), stf_of(s), posrecs, nullptr,
+                                   observed + s * s_obs, &Js, nullptr, checkpoint_every,
+                                   nullptr, nullptr, sum);
+    if (rc) return rc;
+    J += Js;  // shot order
+  }
+  ADJ_TRY(ctx, awc::copy_to_host(ctx, grad_c2, sum, N * sizeof(double), st));
+  *misfit = J;
+  return AWC_OK;
 }
 
 int awc_adjoint_sources(awc_ctx* ctx, const awc_problem* p, const double* vel,

@@ -535,40 +535,42 @@ int plan_upload(awc_plan* P, const double* vel, const double* coeffs, const int6
   cudaStream_t st = C->stream;
   const int64_t h = p->halo, nt = p->nt, nsrc = p->nsrc, nrec = p->nrec;
   const bool f64 = p->precision == AWC_F64;
-  // fact = dt^2 vel^2 on the device in FP64, written pitched
-  CUDA_TRY(err, awc::copy_to_device(C, P->staging, vel, P->N * 8, st));
-  {
-    const double dt2 = p->dt * p->dt;
-    const int blocks = grid_for(C, P->N, 256);
-    if (f64)
-      awc::make_fact<double><<<blocks, 256, 0, st>>>(P->staging, (double*)P->fact, dt2, P->N,
-                                                     p->nx, P->px);
-    else
-      awc::make_fact<float><<<blocks, 256, 0, st>>>(P->staging, (float*)P->fact, dt2, P->N,
-                                                    p->nx, P->px);
-    CUDA_TRY(err, cudaGetLastError());
-  }
-  // coefficients (and which band sides are live)
-  const int64_t clen = awc_coeffs_len(p);
   std::vector<unsigned char> tmp;
-  if (f64) to_T<double>(coeffs, tmp, clen); else to_T<float>(coeffs, tmp, clen);
-  CUDA_TRY(err, cudaMemcpyAsync(P->coef, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, st));
-  CUDA_TRY(err, cudaStreamSynchronize(st));  // tmp is reused below
-  for (int a = 0; a < p->ndim; ++a) {
-    const double* blk = coeffs + a * (8 * h + 4);
-    for (int s = 0; s < 2; ++s) {
-      // a side whose every a is 0 and every b/K is 1 keeps ψ = ξ = 0 for ever
-      // (the free top, acoustic_3D_xPU.jl:225-230); its updates are skipped.
-      bool trivial = true;
-      for (int64_t m = 0; m < h; ++m)
-        trivial = trivial && blk[s * h + m] == 0.0 && blk[2 * h + s * h + m] == 1.0;
-      const double* hb = blk + 4 * h;
-      for (int64_t m = 0; m < h + 1; ++m)
-        trivial = trivial && hb[s * (h + 1) + m] == 0.0 && hb[2 * (h + 1) + s * (h + 1) + m] == 1.0;
-      P->active[a][s] = (h > 0 && !trivial) ? 1 : 0;
+  if (vel) {  // NULL: a new shot over the model already uploaded
+    // fact = dt^2 vel^2 on the device in FP64, written pitched
+    CUDA_TRY(err, awc::copy_to_device(C, P->staging, vel, P->N * 8, st));
+    {
+      const double dt2 = p->dt * p->dt;
+      const int blocks = grid_for(C, P->N, 256);
+      if (f64)
+        awc::make_fact<double><<<blocks, 256, 0, st>>>(P->staging, (double*)P->fact, dt2, P->N,
+                                                       p->nx, P->px);
+      else
+        awc::make_fact<float><<<blocks, 256, 0, st>>>(P->staging, (float*)P->fact, dt2, P->N,
+                                                      p->nx, P->px);
+      CUDA_TRY(err, cudaGetLastError());
     }
+    // coefficients (and which band sides are live)
+    const int64_t clen = awc_coeffs_len(p);
+    if (f64) to_T<double>(coeffs, tmp, clen); else to_T<float>(coeffs, tmp, clen);
+    CUDA_TRY(err, cudaMemcpyAsync(P->coef, tmp.data(), tmp.size(), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(err, cudaStreamSynchronize(st));  // tmp is reused below
+    for (int a = 0; a < p->ndim; ++a) {
+      const double* blk = coeffs + a * (8 * h + 4);
+      for (int s = 0; s < 2; ++s) {
+        // a side whose every a is 0 and every b/K is 1 keeps ψ = ξ = 0 for ever
+        // (the free top, acoustic_3D_xPU.jl:225-230); its updates are skipped.
+        bool trivial = true;
+        for (int64_t m = 0; m < h; ++m)
+          trivial = trivial && blk[s * h + m] == 0.0 && blk[2 * h + s * h + m] == 1.0;
+        const double* hb = blk + 4 * h;
+        for (int64_t m = 0; m < h + 1; ++m)
+          trivial = trivial && hb[s * (h + 1) + m] == 0.0 && hb[2 * (h + 1) + s * (h + 1) + m] == 1.0;
+        P->active[a][s] = (h > 0 && !trivial) ? 1 : 0;
+      }
+    }
+    if (p->ndim == 3) make_regions(P);
   }
-  if (p->ndim == 3) make_regions(P);
   P->tb_io_shape = ~0ull;
   // every node carrying sources and/or receivers, in first-appearance order
   // (sources first); its sources are summed in source order
@@ -1539,6 +1541,21 @@ int plan_for(awc_ctx* C, awc_plan** slot, const awc_problem* p, const double* ve
   P = *slot;
   if ((rc = awc_plan_autotune(P, C->autotune_steps, nullptr))) return rc;
   P->depth = 1;
+  return awc_plan_reset(P);
+}
+
+int plan_shot(awc_ctx* C, awc_plan* P, const int64_t* possrcs, const double* dt2srctf,
+              const int64_t* posrecs) {
+  const awc_problem* p = &P->p;
+  int rc;
+  if ((rc = check_positions(p, possrcs, p->nsrc, "source", &C->err)) ||
+      (rc = check_positions(p, posrecs, p->nrec, "receiver", &C->err)))
+    return rc;
+  if (p->nsrc > 0 && p->nt > 0 && !dt2srctf)
+    return set_err(&C->err, AWC_ERR_INVALID, "dt2srctf is NULL");
+  CUDA_TRY(&C->err, cudaSetDevice(C->device));
+  P->depth = 1;
+  if ((rc = plan_upload(P, nullptr, nullptr, possrcs, dt2srctf, posrecs))) return rc;
   return awc_plan_reset(P);
 }
 

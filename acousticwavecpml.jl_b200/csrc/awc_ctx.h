@@ -72,6 +72,10 @@ void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t coun
 int plan_for(awc_ctx* C, awc_plan** slot, const awc_problem* p, const double* vel,
              const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
              const int64_t* posrecs, bool tune = false);
+// Replaces the sources and receivers of plan P (its model, fact and CPML
+// coefficients kept) and resets it: the next shot over the same model.
+int plan_shot(awc_ctx* C, awc_plan* P, const int64_t* possrcs, const double* dt2srctf,
+              const int64_t* posrecs);
 
 // Host <-> device copies that return once complete. Large pageable host
 // buffers go through the context's pinned staging buffer, the host side of

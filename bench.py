@@ -384,10 +384,12 @@ def batch_profile_run(args, local):
 def gradient_leg(pkg, ctx, rank, world, timed_host):
     """3D gradient, FP32 with an FP64 check: config 4's 16 shots, dJ/d(c²)
     summed over the shots at the initial model against the true model's
-    traces of the same precision, through awc_misfit_gradient (host buffers,
-    checkpoint every 50 steps, nt = 1500). Rank r takes shots r, r + N, ...;
+    traces of the same precision, through awc_misfit_gradient_shots (host
+    buffers, checkpoint every 50 steps, nt = 1500; one call per rank, the
+    shots' gradients summed on the device). Rank r takes shots r, r + N, ...;
     under torchrun the ranks' sums are added with one all-reduce
-    (adjoint.sharded_gradient). The FP64 build checks shot 0."""
+    (adjoint.sharded_gradient). Also timed: one awc_misfit_gradient call per
+    shot for two shots. The FP64 build checks shot 0."""
     import time
     import torch
     import torch.distributed as dist
@@ -419,15 +421,28 @@ def gradient_leg(pkg, ctx, rank, world, timed_host):
     t_fwd = time.perf_counter() - t0
     adjoint.misfit_gradient(si0, obs0, w["checkpoint_every"], ctx)  # warm-up
 
-    def one_shot(k):
-        _, si, obs = data[k]
-        J, g, _ = adjoint.misfit_gradient(si, obs, w["checkpoint_every"], ctx)
-        return J, g
+    # the rank's shots share one velocity array, and their observed traces
+    # are stacked (nt x nrec x shots) before the timed region
+    for k in mine:
+        data[k][1]["vel"] = si0["vel"]
+    obs_all = np.asfortranarray(np.stack([data[k][2] for k in mine], axis=-1)) if mine else None
+
+    def shots_of(ks):
+        return adjoint.misfit_gradient_shots([data[k][1] for k in ks],
+                                             obs_all if ks == mine else [data[k][2] for k in ks],
+                                             w["checkpoint_every"], ctx)
 
     out = {}
     t_grad = timed_host(lambda: out.update(
-        r=adjoint.sharded_gradient(list(range(nshot)), one_shot, w["init"].shape)))
+        r=adjoint.sharded_gradient(list(range(nshot)), shots_of, w["init"].shape,
+                                   batched=True)))
     J32_all, g32_all = out["r"]
+    # one call per shot (rank 0's first two shots), for comparison
+    k2 = (mine or [0])[:2]
+    t0 = time.perf_counter()
+    for k in k2:
+        adjoint.misfit_gradient(data[k][1], data[k][2], w["checkpoint_every"], ctx)
+    t_single = (time.perf_counter() - t0) / len(k2)
     # FP64 check on shot 0 (rank 0), against its own FP64 data; and the FP32
     # adjoint given the FP64 residual, which separates the adjoint's own
     # rounding from the residual's (a small difference of two FP32 traces)
@@ -448,6 +463,8 @@ def gradient_leg(pkg, ctx, rank, world, timed_host):
             "value": nshot / t_grad, "unit": "shot gradients/s",
             "s_for_all_shots": t_grad, "s_per_gradient": t_grad * world / nshot,
             "s_per_forward": t_fwd, "gradient_over_forward": t_grad * world / nshot / t_fwd,
+            "s_per_gradient_one_call_per_shot": t_single,
+            "one_call_per_shot_over_forward": t_single / t_fwd,
             "misfit_all_shots": float(J32_all), "checkpoint_every": w["checkpoint_every"],
             "nt": p.nt, "grid": [p.nx, p.ny, p.nz], **res,
             "check_shot": 0,

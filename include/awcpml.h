@@ -292,6 +292,20 @@ int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
                         const int64_t* posrecs, const double* observed, int32_t checkpoint_every,
                         double* misfit, double* grad_c2, double* traces);
 
+/* awc_misfit_gradient summed over `nshot` shots of one model (the sum of
+ * the shots' J and of their dJ/d(c²), each shot's as awc_misfit_gradient
+ * returns it, added in shot order): vel is uploaded once, the gradients
+ * are summed on the device and read back once. The shots share p (so the
+ * same nsrc, nrec and nt), vel, coeffs and posrecs; shot s reads
+ * possrcs + s*nsrc*ndim (nsrc x ndim), dt2srctf + s*nt*nsrc (nt x nsrc) and
+ * observed + s*nt*nrec (nt x nrec). Replaces a caller-side loop of
+ * awc_misfit_gradient calls over the shots of one source survey. */
+int awc_misfit_gradient_shots(awc_ctx* ctx, const awc_problem* p, int32_t nshot,
+                              const double* vel, const double* coeffs, const int64_t* possrcs,
+                              const double* dt2srctf, const int64_t* posrecs,
+                              const double* observed, int32_t checkpoint_every, double* misfit,
+                              double* grad_c2);
+
 /* The transpose of the linear map from injected source values (dt2srctf,
  * nt x nsrc) to traces (nt x nrec) for fixed c: src_out (nt x nsrc) =
  * Aᵀ adjoint_traces. Sources and receivers on the Dirichlet rim have no

@@ -7,6 +7,7 @@
   forward (eps = 1e-4 relative, 20 cells in 2D, 10 in 3D, dt fixed), 1e-6.
 * The checkpoint interval does not change the gradient (bitwise); the FP32
   gradient follows the FP64 one (relative L2 <= 1e-4).
+* The multi-shot call is bitwise the sum of the single-shot calls.
 * A source on the Dirichlet rim: the gradient next to it against central
   differences."""
 import numpy as np
@@ -219,6 +220,54 @@ def test_fp32_gradient_follows_fp64(pkg, ctx, dim):
     print(f"{dim}D fp32 gradient rel-L2 {e:.3e}, misfit {J32:.6e} vs {J64:.6e}")
     assert e <= 1e-4
     assert abs(J32 - J64) <= 1e-4 * J64
+
+
+@pytest.mark.parametrize("dim,precision", [(2, "f64"), (3, "f32"), (3, "f64")])
+def test_misfit_gradient_shots_is_the_sum_of_shots(pkg, ctx, dim, precision):
+    """awc_misfit_gradient_shots (the model uploaded once, the gradients summed
+    on the device) equals summing awc_misfit_gradient over the shots in order,
+    bitwise, J and gradient; the shots move the two sources around the grid
+    (band and core nodes), with observed data from another model."""
+    from acousticwavecpml_b200 import adjoint
+    rng = np.random.default_rng(40 + dim)
+    L, vel, srcs, recs, kw = (model2d if dim == 2 else model3d)(rng)
+    d = 10.0
+    n = vel.shape
+    moves = [(0, 0), (5, -2), (-9, 3), (11, 7)]
+    setups, obs = [], []
+    true = np.asfortranarray(vel * (1.0 + 0.02 * rng.standard_normal(vel.shape)))
+    for mx, my in moves:
+        sh = [[min(max(c[0] + mx * d, 2 * d), (n[0] - 3) * d),
+               min(max(c[1] + my * d, 2 * d), (n[1] - 3) * d)] + list(c[2:]) for c in srcs]
+        s = setup(pkg, L, vel, sh, recs, kw, precision, nt=90)
+        setups.append(s)
+        obs.append(traces_of(ctx, dict(s, vel=true)))
+    J_ref, g_ref = 0.0, np.zeros(vel.shape, order="F")
+    for s, o in zip(setups, obs):
+        j, g, _ = adjoint.misfit_gradient(s, o, 25, ctx)
+        J_ref += j
+        g_ref += g
+    J, g = adjoint.misfit_gradient_shots(setups, obs, 25, ctx)
+    assert J == J_ref
+    assert np.array_equal(g, g_ref)
+    assert np.abs(g_ref).max() > 0
+    # one shot: the single-shot call's own result
+    j0, g0, _ = adjoint.misfit_gradient(setups[2], obs[2], 25, ctx)
+    J1, g1 = adjoint.misfit_gradient_shots(setups[2:3], obs[2:3], 25, ctx)
+    assert J1 == j0 and np.array_equal(g1, g0)
+
+
+def test_misfit_gradient_shots_rejects_mixed_shots(pkg, ctx):
+    from acousticwavecpml_b200 import adjoint
+    rng = np.random.default_rng(44)
+    L, vel, srcs, recs, kw = model2d(rng)
+    a = setup(pkg, L, vel, srcs, recs, kw, nt=60)
+    b = setup(pkg, L, vel * 1.01, srcs, recs, kw, nt=60)
+    o = np.zeros((60, a["problem"].nrec))
+    with pytest.raises(ValueError):
+        adjoint.misfit_gradient_shots([a, b], [o, o], 20, ctx)
+    with pytest.raises(ValueError):
+        adjoint.misfit_gradient_shots([a, a], [o], 20, ctx)
 
 
 def test_torch_autograd_function(pkg, ctx):

@@ -118,7 +118,22 @@ def _real_worker(rank, world, port, out):
 
         traces = pkg.solve_sharded(shots, run)
         J, grad = pkg.adjoint.sharded_gradient(shots, _oracle_shot_gradient, (41, 31))
+        batches = []
+
+        def batch(mine):
+            # the rank's shots in one call, summed in order (as
+            # misfit_gradient_shots does on the device)
+            batches.append([s["src"][0][0] for s in mine])
+            Jb, gb = 0.0, np.zeros((41, 31), order="F")
+            for s in mine:
+                j, g = _oracle_shot_gradient(s)
+                Jb += j
+                gb += g
+            return Jb, gb
+
+        Jb, gradb = pkg.adjoint.sharded_gradient(shots, batch, (41, 31), batched=True)
         np.savez(os.path.join(out, f"r{rank}.npz"), J=J, grad=grad, ran=np.array(ran),
+                 Jb=Jb, gradb=gradb, batches=np.array(batches),
                  **{f"t{k}": t for k, t in enumerate(traces)})
     finally:
         dist.destroy_process_group()
@@ -128,8 +143,9 @@ def test_sharded_shots_and_gradient_with_oracle_gloo(tmp_path):
     """Two gloo ranks run the package's shot sharding (batch.shard via
     solve_sharded: rank r takes shots r, r + 2, ...; results gathered in shot
     order) and sharded_gradient (one all-reduce of [gradient, misfit]) with
-    per-shot functions that run the oracle. Both ranks must end with what a
-    single process computes for the whole set."""
+    per-shot functions that run the oracle, per shot and batched (one call per
+    rank with its shots). Both ranks must end with what a single process
+    computes for the whole set."""
     import torch.multiprocessing as mp
     mp.spawn(_real_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
     shots = _oracle_shots()
@@ -144,8 +160,12 @@ def test_sharded_shots_and_gradient_with_oracle_gloo(tmp_path):
         d = np.load(tmp_path / f"r{r}.npz")
         for k, t in enumerate(ref_tr):
             np.testing.assert_array_equal(d[f"t{k}"], t)
-        assert abs(float(d["J"]) - J_ref) <= 1e-12 * J_ref
-        np.testing.assert_allclose(d["grad"], g_ref, rtol=1e-12, atol=1e-30)
+        for J, g in ((d["J"], d["grad"]), (d["Jb"], d["gradb"])):
+            assert abs(float(J) - J_ref) <= 1e-12 * J_ref
+            np.testing.assert_allclose(g, g_ref, rtol=1e-12, atol=1e-30)
+        # one batched call per rank, with the rank's shots in order
+        assert d["batches"].shape[0] == 1
+        assert list(d["batches"][0]) == [s["src"][0][0] for s in shots[r::2]]
         ran += list(d["ran"])
     # each shot ran on exactly one rank
     assert sorted(ran) == sorted(s["src"][0][0] for s in shots)
