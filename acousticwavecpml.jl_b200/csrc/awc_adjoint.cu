@@ -25,7 +25,8 @@
 //     w_q = a_{q-1} ν_{t+1}[q-1] + F(c_q) λ_{t+1}(c_q) (0 outside q = 1..h),
 // and dJ/dF(c) = Σ_t λ_{t+1}(c) B_t(c), where B_t is the bracket multiplying
 // F. At a node outside every active CPML band that bracket is the Laplacian
-// of p_t, Σ_axes D2 p_t(c), evaluated from the stored p_t in double; inside
+// of p_t, Σ_axes D2 p_t(c), evaluated from the stored p_t in the working
+// precision; inside
 // a band it also holds the ψ and ξ terms, and B_t = (p_{t+1} - 2 p_t + p_{t-1}
 // - S_t)(c) / F(c) there. (The difference form divides a second difference
 // in time, about (ω dt)² ≈ 1e-3 of p, by F, and at a source node subtracts
@@ -860,7 +861,6 @@ constexpr int adj_core_smem() {
   return ADJ_STAGES * awc::AdjTile<T, ADJ_TY>::BYTES + 2 * ADJ_STAGES * 8 + 16;
 }
 
-// Tensor map of a pitched field for the TMA core kernel's boxes.
 // Tensor map of a pitched field (elements of type E) for the TMA core
 // kernel: the box with a ring (ring = true) or the tile.
 template <typename T, typename E = T>
@@ -1071,6 +1071,9 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
       for (int64_t m = 0; m < nfield; ++m)
         seg[b][m] = arena + nseg * chk_elems + (b * nfield + m) * NP;
     }
+    // the steps write the segment fields in place, interior nodes only: the
+    // rims stay zero
+    ADJ_TRY(C, cudaMemsetAsync(seg[0][0], 0, nset * nfield * NP * sizeof(T), st));
   }
   // tensor maps of the TMA-fed core kernel: both λ buffers, F, every segment field
   CUtensorMap map_lam[2], map_lam3[2], map_f, map_grad;
@@ -1117,7 +1120,7 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
         std::vector<T*>& f = seg[c % nset];
         ADJ_TRY(C, cudaMemcpyAsync(f[0], V.buf[s % 3], fb, cudaMemcpyDeviceToDevice, st));
         ADJ_TRY(C, cudaMemcpyAsync(f[1], V.buf[(s + 1) % 3], fb, cudaMemcpyDeviceToDevice, st));
-        awc::plan_keep_fields(plan, (void* const*)(f.data() + 2), s, e - s);
+        awc::plan_keep_fields(plan, (void* const*)(f.data() + 2), s, e - s, true);
       }
       rc = awc_plan_run(plan, e - s, 1, nullptr);
       awc::plan_keep_fields(plan, nullptr, 0, 0);
@@ -1163,7 +1166,7 @@ int adjoint_impl(awc_ctx* C, awc_plan* plan, const awc_problem* p, const double*
     awc::plan_set_step(plan, s);
     ADJ_TRY(C, cudaMemcpyAsync(seg[b][0], V.buf[s % 3], fb, cudaMemcpyDeviceToDevice, st));
     ADJ_TRY(C, cudaMemcpyAsync(seg[b][1], V.buf[(s + 1) % 3], fb, cudaMemcpyDeviceToDevice, st));
-    awc::plan_keep_fields(plan, (void* const*)(seg[b].data() + 2), s, e - s);
+    awc::plan_keep_fields(plan, (void* const*)(seg[b].data() + 2), s, e - s, true);
     r = awc_plan_run(plan, e - s, 1, nullptr);
     awc::plan_keep_fields(plan, nullptr, 0, 0);
     if (r) return r;

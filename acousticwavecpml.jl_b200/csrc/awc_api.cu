@@ -339,11 +339,16 @@ struct awc_plan {
       return true;
     }
   } graph_key;
-  // copy of each new field to keep: after step it in [keep_first,
-  // keep_first + keep_count) the new field goes to keep[it - keep_first]
-  // (eager runs only; set by the adjoint's segment recompute)
+  // fields to keep: the new field of step it in [keep_first, keep_first +
+  // keep_count) goes to keep[it - keep_first] (set by the adjoint's forward
+  // run and segment recompute). Copied after the step, or, with keep_in_place,
+  // written there by the step itself, which then reads p_{it-1} and p_it from
+  // keep[m - 2] and keep[m - 1] (m = it - keep_first; keep[-2] and keep[-1]
+  // hold the fields before the range), the plan's buffers refreshed after
+  // the range's last step.
   void* const* keep = nullptr;
   int64_t keep_first = 0, keep_count = 0;
+  bool keep_in_place = false;
 
   int alloc(void** out, size_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -888,12 +893,12 @@ int ensure_io(awc_plan* P) {
 // Tensor maps of the 3D core kernel: for each rotating field buffer a map
 // with the pcur box ((64 + 2A) x (by + 2) x 1) and one with the pold box
 // (64 x by x 1), and one for fact. Dims (nx, ny, nz), pitched strides.
-int ensure_maps(awc_plan* P) {
-  if (P->maps_by == P->by) return AWC_OK;
-  awc_ctx* C = P->ctx;
-  const awc_problem* p = &P->p;
+// Tensor map of a pitched field of the plan for the core kernel at the
+// current tile height: the box with its ring (ring = true) or the tile.
+bool field_map(const awc_plan* P, CUtensorMap* m, const void* base, bool ring) {
   PFN_cuTensorMapEncodeTiled_v12000 enc = awc::tensor_map_encoder();
-  if (!enc) return set_err(&C->err, AWC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  if (!enc) return false;
+  const awc_problem* p = &P->p;
   const bool f64 = p->precision == AWC_F64;
   const CUtensorMapDataType dt = f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   const cuuint32_t A = 16 / (cuuint32_t)P->esz;
@@ -902,15 +907,20 @@ int ensure_maps(awc_plan* P) {
   const cuuint32_t box_c[3] = {64 + 2 * A, (cuuint32_t)P->by + 2, 1};
   const cuuint32_t box_i[3] = {64, (cuuint32_t)P->by, 1};
   const cuuint32_t es[3] = {1, 1, 1};
-  auto make = [&](CUtensorMap* m, void* base, const cuuint32_t* box) -> bool {
-    return enc(m, dt, 3, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-  };
+  return enc(m, dt, 3, const_cast<void*>(base), dims, strides, ring ? box_c : box_i, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int ensure_maps(awc_plan* P) {
+  if (P->maps_by == P->by) return AWC_OK;
+  awc_ctx* C = P->ctx;
+  if (!awc::tensor_map_encoder())
+    return set_err(&C->err, AWC_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
   for (int b = 0; b < P->nbuf; ++b)
-    if (!make(&P->map_c[b], P->buf[b], box_c) || !make(&P->map_o[b], P->buf[b], box_i))
+    if (!field_map(P, &P->map_c[b], P->buf[b], true) || !field_map(P, &P->map_o[b], P->buf[b], false))
       return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
-  if (!make(&P->map_f, P->fact, box_i))
+  if (!field_map(P, &P->map_f, P->fact, false))
     return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
   P->maps_by = P->by;
   return AWC_OK;
@@ -1112,10 +1122,19 @@ int init_kernel_attrs(std::string* err) {
 }
 
 template <typename T, int TY>
-void launch_core(awc_plan* P, const StepState& stt, const awc::StepParams<T>& S, dim3 grid,
-                 cudaStream_t st) {
+void launch_core(awc_plan* P, const CUtensorMap& mc, const CUtensorMap& mo,
+                 const awc::StepParams<T>& S, dim3 grid, cudaStream_t st) {
   awc::step3d_core<T, TY, stages<T>()><<<grid, dim3(32, TY), core_smem<T, TY>(), st>>>(
-      P->map_c[stt.ord[0]], P->map_o[stt.ord[1]], P->map_f, S);
+      mc, mo, P->map_f, S);
+}
+
+// Whether step it writes its field into the keep list itself: only when no
+// source or receiver sits on the rim, whose values (p_{t+1} = p_{t-1} + S_t
+// there) the step reads from the buffer it overwrites; the keep list's rims
+// are zero, as the plan's are without rim sources.
+bool kept_in_place(const awc_plan* P, int64_t it) {
+  return P->keep && P->keep_in_place && P->io_nrim == 0 && it >= P->keep_first &&
+         it < P->keep_first + P->keep_count;
 }
 
 // One time step. 3D: the shell kernel on the context's second stream and the
@@ -1126,6 +1145,21 @@ int launch_step(awc_plan* P, int64_t it, const StepState& stt, cudaStream_t st) 
   awc_ctx* C = P->ctx;
   const awc_problem* p = &P->p;
   awc::StepParams<T> S = step_params<T>(P, it, stt);
+  const CUtensorMap* mc = &P->map_c[stt.ord[0]];
+  const CUtensorMap* mo = &P->map_o[stt.ord[1]];
+  CUtensorMap kc, ko;
+  if (kept_in_place(P, it)) {
+    void* const* f = P->keep + (it - P->keep_first);
+    S.pold = (const T*)f[-2];
+    S.pcur = (const T*)f[-1];
+    S.pnew = (T*)f[0];
+    if (p->ndim == 3 && P->has_core) {
+      if (!field_map(P, &kc, f[-1], true) || !field_map(P, &ko, f[-2], false))
+        return set_err(&C->err, AWC_ERR_CUDA, "tensor map encoding failed");
+      mc = &kc;
+      mo = &ko;
+    }
+  }
   if (p->ndim == 2) {
     kernel_params(P, 0, S);
     awc::step2d<T><<<step_grid(P), dim3(32, 8), 0, st>>>(S);
@@ -1150,9 +1184,9 @@ int launch_step(awc_plan* P, int64_t it, const StepState& stt, cudaStream_t st) 
       kernel_params(P, 0, S);
       const dim3 grid = step_grid(P);
       switch (P->by) {
-        case 4: launch_core<T, 2>(P, stt, S, grid, st); break;
-        case 8: launch_core<T, 4>(P, stt, S, grid, st); break;
-        case 16: launch_core<T, 8>(P, stt, S, grid, st); break;
+        case 4: launch_core<T, 2>(P, *mc, *mo, S, grid, st); break;
+        case 8: launch_core<T, 4>(P, *mc, *mo, S, grid, st); break;
+        case 16: launch_core<T, 8>(P, *mc, *mo, S, grid, st); break;
         default: return set_err(&C->err, AWC_ERR_INVALID, "unsupported tile height %d", P->by);
       }
     }
@@ -1278,10 +1312,18 @@ int launch_range(awc_plan* P, int64_t start, int64_t n, StepState& stt, cudaStre
     }
     rc = f64 ? launch_step<double>(P, it, stt, st) : launch_step<float>(P, it, stt, st);
     if (rc) return rc;
-    if (P->keep && it >= P->keep_first && it < P->keep_first + P->keep_count)
+    const bool in_place = kept_in_place(P, it);
+    if (P->keep && !in_place && it >= P->keep_first && it < P->keep_first + P->keep_count)
       CUDA_TRY(&P->ctx->err, cudaMemcpyAsync(P->keep[it - P->keep_first], P->buf[stt.ord[2]],
                                              P->NP * P->esz, cudaMemcpyDeviceToDevice, st));
     stt.step1();
+    if (in_place && it == P->keep_first + P->keep_count - 1) {
+      // the plan's buffers take p_it and p_{it+1} back from the keep list
+      void* const* f = P->keep + (it - P->keep_first);
+      const size_t fb = P->NP * P->esz;
+      CUDA_TRY(&P->ctx->err, cudaMemcpyAsync(P->buf[stt.ord[0]], f[0], fb, cudaMemcpyDeviceToDevice, st));
+      CUDA_TRY(&P->ctx->err, cudaMemcpyAsync(P->buf[stt.ord[1]], f[-1], fb, cudaMemcpyDeviceToDevice, st));
+    }
     ++it;
   }
   return AWC_OK;
@@ -1339,9 +1381,12 @@ int get_graph(awc_plan* P, int64_t start, int64_t n, cudaGraphExec_t* out) {
     uint64_t hsh = 1469598103934665603ull;  // FNV-1a over the destinations in range
     for (int64_t it = std::max(start, P->keep_first);
          it < std::min(start + n, P->keep_first + P->keep_count); ++it) {
-      hsh ^= (uint64_t)(uintptr_t)P->keep[it - P->keep_first];
-      hsh *= 1099511628211ull;
+      for (int64_t d = P->keep_in_place ? -2 : 0; d <= 0; ++d) {  // in place: the fields read too
+        hsh ^= (uint64_t)(uintptr_t)P->keep[it - P->keep_first + d];
+        hsh *= 1099511628211ull;
+      }
     }
+    hsh ^= P->keep_in_place ? 0x9e3779b97f4a7c15ull : 0ull;
     kh = (int64_t)(hsh | 1);
   }
   const std::array<int64_t, 5> gk{start, n, P->state.code(), kfirst, kh};
@@ -1564,10 +1609,12 @@ void plan_set_step(awc_plan* P, int64_t step) {
   P->state = StepState::after_steps(step);
 }
 
-void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count) {
+void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count,
+                      bool in_place) {
   P->keep = dst;
   P->keep_first = first;
   P->keep_count = dst ? count : 0;
+  P->keep_in_place = dst && in_place;
 }
 }  // namespace awc
 

@@ -61,9 +61,15 @@ struct PlanView {
 PlanView plan_view(awc_plan* P);
 // Sets the step counter of a plan whose state was restored from a copy.
 void plan_set_step(awc_plan* P, int64_t step);
-// During eager runs, copies the new field of each step it in [first,
-// first + count) to dst[it - first] (stream-ordered); NULL stops it.
-void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count);
+// Keeps the new field of each step it in [first, first + count) in
+// dst[it - first]: a stream-ordered copy after the step, or, in place (when
+// the shot has no source or receiver on the rim; else copied), the step
+// writes it there and reads p_{it-1}, p_it from dst[it - first - 2],
+// dst[it - first - 1] (dst[-2] and dst[-1] must hold p_{first-1} and
+// p_first, and every dst field a zero rim); the plan's own buffers are
+// refreshed after the last step. NULL stops it.
+void plan_keep_fields(awc_plan* P, void* const* dst, int64_t first, int64_t count,
+                      bool in_place = false);
 
 // Re-uploads a new shot into *slot when it holds a plan of the same shape
 // (same buffers), else replaces it by a new plan, whose 3D launch shape is

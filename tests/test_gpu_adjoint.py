@@ -192,11 +192,14 @@ def test_gradient_with_rim_source_vs_oracle_fd(pkg, oracle, ctx):
         assert abs(grad[cell] - fd) <= 1e-6 * max(abs(fd), 1e-3 * np.abs(grad).max())
 
 
-def test_checkpoint_interval_is_exact(pkg, ctx):
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_checkpoint_interval_is_exact(pkg, ctx, precision):
+    """Every checkpoint interval gives the same gradient, bit for bit, in
+    both precisions."""
     from acousticwavecpml_b200 import adjoint
     rng = np.random.default_rng(5)
     L, vel, srcs, recs, kw = model3d(rng, freetop=False)
-    s = setup(pkg, L, vel, srcs, recs, kw, nt=90)
+    s = setup(pkg, L, vel, srcs, recs, kw, precision, nt=90)
     obs = np.zeros((90, s["problem"].nrec))
     ref = adjoint.misfit_gradient(s, obs, checkpoint_every=90, ctx=ctx)[1]
     for k in (1, 7, 50):
