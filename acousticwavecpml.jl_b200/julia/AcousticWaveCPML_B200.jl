@@ -21,7 +21,7 @@ module AcousticWaveCPML_B200
 
 import ..AcousticWaveCPML: Sources, Receivers, calc_Kab_CPML
 
-export solve1D, solve2D, solve3D, misfit, misfit_gradient
+export solve1D, solve2D, solve3D, misfit, misfit_gradient, misfit_gradient_shots
 
 const LIBAWCPML = get(ENV, "AWCPML_LIB", joinpath(@__DIR__, "..", "lib", "libawcpml.so"))
 
@@ -252,6 +252,57 @@ function misfit_gradient(ls::NTuple{N,Real}, vel::Array{<:Real,N}, srcs::Sources
                Int32(checkpoint_every), J, grad, traces)
     check(rc, ctx)
     recs.seismograms = traces
+    return J[], grad
+end
+
+"""
+    misfit_gradient_shots(ls, vel, shots, recs, observed; dt, nt, halo=20, rcoef=0.0001,
+                          freetop=true, precision=:f64, checkpoint_every=50, device=0)
+
+Σ over the shots (a vector of `Sources` with the same number of sources and
+the same frequency, over one model and one receiver set; `observed[s]` is shot
+s's nt x nrec data) of the misfit and dJ/d(c²): one call of
+`awc_misfit_gradient_shots`, which uploads the model once and sums the
+gradients on the device; equal to summing `misfit_gradient` over the shots.
+No counterpart in the reference.
+"""
+function misfit_gradient_shots(ls::NTuple{N,Real}, vel::Array{<:Real,N}, shots::Vector{Sources},
+                               recs::Receivers, observed::Vector{Matrix{Float64}}; dt::Real,
+                               nt::Integer, halo::Integer=20, rcoef::Real=0.0001,
+                               freetop::Bool=true, precision::Symbol=:f64,
+                               checkpoint_every::Integer=50, device::Integer=0) where {N}
+    nshot = length(shots)
+    nshot == length(observed) || error("one observed matrix per shot")
+    nsrc = shots[1].n
+    all(s -> s.n == nsrc, shots) || error("every shot needs the same number of sources")
+    f0 = shots[1].freqdomain
+    vel_max = maximum(vel)
+    ns = size(vel)
+    ds = ntuple(a -> ls[a] / (ns[a] - 1), N)
+    times = collect(range(0.0, step=dt, length=nt))
+    snap(pos) = round.(Int64, pos ./ reshape(collect(ds), 1, N) .+ 1, RoundNearestTiesUp)
+    possrcs = zeros(Int64, nsrc, N, nshot)
+    dt2srctf = zeros(nt, nsrc, nshot)
+    for (k, srcs) in enumerate(shots)
+        possrcs[:, :, k] .= snap(srcs.positions)
+        for s = 1:nsrc
+            dt2srctf[:, s, k] .= (dt^2 / prod(ds)) .* srcs.srctfs[s].(times, srcs.t0s[s], f0)
+        end
+    end
+    obs = cat(observed...; dims=3)
+    coeffs = packed_coeffs(halo, dt, ds, vel_max, rcoef, f0, freetop)
+    prob = AwcProblem(Int32(N), precision == :f32 ? AWC_F32 : AWC_F64, ns[1], ns[2],
+                      N == 3 ? ns[3] : 1, Int32(halo), Int32(freetop), ds[1], ds[2],
+                      N == 3 ? ds[3] : 1.0, Float64(dt), nt, nsrc, recs.n)
+    J = Ref{Float64}(0.0)
+    grad = zeros(Float64, ns)
+    ctx = context(device)
+    rc = ccall((:awc_misfit_gradient_shots, LIBAWCPML), Cint,
+               (Ptr{Cvoid}, Ref{AwcProblem}, Int32, Ptr{Float64}, Ptr{Float64}, Ptr{Int64},
+                Ptr{Float64}, Ptr{Int64}, Ptr{Float64}, Int32, Ref{Float64}, Ptr{Float64}),
+               ctx, prob, Int32(nshot), Array{Float64}(vel), coeffs, possrcs, dt2srctf,
+               snap(recs.positions), obs, Int32(checkpoint_every), J, grad)
+    check(rc, ctx)
     return J[], grad
 end
 
