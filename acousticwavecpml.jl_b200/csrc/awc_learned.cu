@@ -13,6 +13,14 @@
 //       r = c dt / d along the normal (K = 3 * 3^d + 1: 28 in 2D, 82 in 3D;
 //       without r a local operator cannot tell how fast the wave leaves),
 //       weights in BF16, products accumulated in FP32.
+// The two hidden layers run on the tensor cores (mma.sync m16n8k16, BF16
+// operands, FP32 accumulation): a warp takes 16 layer nodes at a time, the
+// weights are B operands as they are, and each FP32 activation enters as
+// the sum of three BF16 terms (hi + mid + lo, three MMAs), which carries its
+// 24 bits: the products are those of the FP32 activations with the BF16
+// weights, accumulated in FP32 (a BF16-rounded activation would change the
+// solution by up to 5e-2 relative over a few hundred steps of an unstable
+// layer).
 // A node within W of two sides uses the nearer one (x before y before z on
 // ties). Sources are added after the update, then receivers sample p_{t+1}.
 // FP32 only; rim sources and receivers are rejected.
@@ -29,7 +37,11 @@
 namespace {
 
 constexpr int kHid = 32;
-constexpr int kMaxIn = 82;
+constexpr int kMaxKP = 96;          // K (at most 82) padded to the MMA's k of 16
+constexpr int kWS1 = kMaxKP + 8;    // smem row strides (bf16): conflict-free B loads
+constexpr int kWS2 = kHid + 8;
+constexpr int kXS = kMaxKP + 8;     // smem row stride (floats) of a warp's input tile
+constexpr int kWarps = 4;
 
 struct LearnedParams {
   int32_t ndim, nx, ny, nz, width, freetop;
@@ -43,12 +55,9 @@ struct LearnedParams {
   float* p3;        // p_{t+1}
   const __nv_bfloat16* w;  // W1 (32 x K), b1 (32), W2 (32 x 32), b2 (32), W3 (32), b3 (1)
   int32_t nin;
+  const int4* layer;  // layer nodes (i, j, k, 2 axis + (sign > 0)), memory order
+  int32_t nlayer;
 };
-
-__device__ __forceinline__ bool interior_node(const LearnedParams& L, int i, int j, int k) {
-  return i >= 1 && i <= L.nx - 2 && j >= 1 && j <= L.ny - 2 &&
-         (L.ndim == 2 || (k >= 1 && k <= L.nz - 2));
-}
 
 // Depth (1 = next to the rim) of the nearest absorbing side and its axis and
 // outward sign, or 0 when the node is not in the layer.
@@ -89,70 +98,185 @@ __global__ void __launch_bounds__(256) learned_interior(LearnedParams L) {
   L.p3[o] = fmaf(L.F[o], lap, 2.f * pc - L.p1[o]);
 }
 
-// One thread per interior node; layer nodes run the MLP. The weights are
-// staged in shared memory as floats.
-__global__ void __launch_bounds__(256) learned_layer(LearnedParams L) {
-  __shared__ float w[kHid * kMaxIn + kHid + kHid * kHid + kHid + kHid + 1];
-  const int K = L.nin;
-  const int nw = kHid * K + kHid + kHid * kHid + kHid + kHid + 1;
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  for (int e = tid; e < nw; e += blockDim.x * blockDim.y) w[e] = __bfloat162float(L.w[e]);
-  __syncthreads();
-  const float* W1 = w;
-  const float* b1 = W1 + kHid * K;
-  const float* W2 = b1 + kHid;
-  const float* b2 = W2 + kHid * kHid;
-  const float* W3 = b2 + kHid;
-  const float b3 = W3[kHid];
-  const int i = 1 + blockIdx.x * 32 + threadIdx.x;
-  const int j = 1 + blockIdx.y * 8 + threadIdx.y;
-  const int k = L.ndim == 3 ? 1 + blockIdx.z : 0;
-  if (i > L.nx - 2 || j > L.ny - 2) return;
-  int ax = 0, sg = 1;
-  if (!layer_side(L, i, j, k, ax, sg)) return;
-  // the two transverse axes in increasing order
-  int t1 = -1, t2 = -1;
-  for (int a = 0; a < L.ndim; ++a)
-    if (a != ax) (t1 < 0 ? t1 : t2) = a;
-  float x[kMaxIn];
-  float s = 0.f;
-  const float* lv[3] = {L.p0, L.p1, L.p2};
-  const int nv = L.ndim == 3 ? 3 : 1;
-  int f = 0;
-  for (int l = 0; l < 3; ++l)
-    for (int u = -1; u <= 1; ++u)
-      for (int v = -1; v <= 1; ++v)
-        for (int q = 0; q < nv; ++q) {
-          const int wq = L.ndim == 3 ? q - 1 : 0;
-          int d[3] = {0, 0, 0};
-          d[ax] = sg * u;
-          d[t1] = v;
-          if (t2 >= 0) d[t2] = wq;
-          const int ii = i + d[0], jj = j + d[1], kk = k + d[2];
-          float val = 0.f;
-          if (interior_node(L, ii, jj, kk)) val = lv[l][ii + L.px * jj + L.plane * kk];
-          x[f++] = val;
-          s = fmaxf(s, fabsf(val));
-        }
-  const float inv = s > 0.f ? 1.f / s : 1.f;
-  for (int c = 0; c < f; ++c) x[c] *= inv;
-  x[f] = sqrtf(L.F[i + L.px * j + L.plane * k]) * L.inv_d[ax];  // Courant number
-  float h1[kHid];
-#pragma unroll 4
-  for (int r = 0; r < kHid; ++r) {
-    float acc = b1[r];
-    for (int c = 0; c < K; ++c) acc = fmaf(W1[r * K + c], x[c], acc);
-    h1[r] = fmaxf(acc, 0.f);
-  }
-  float out = b3;
-#pragma unroll 4
-  for (int r = 0; r < kHid; ++r) {
-    float acc = b2[r];
+// D += A B on the tensor cores: m16n8k16, A and B BF16, D and C FP32.
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Two FP32 values as three pairs of BF16 terms (hi, mid, lo), each pair
+// packed low element first: x = hi + mid + lo to within 2^-27 |x|.
+__device__ __forceinline__ void split3(float x0, float x1, uint32_t& hi, uint32_t& mid,
+                                       uint32_t& lo) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(x0, x1);
+  const float r0 = x0 - __low2float(h), r1 = x1 - __high2float(h);
+  const __nv_bfloat162 m = __floats2bfloat162_rn(r0, r1);
+  const __nv_bfloat162 l = __floats2bfloat162_rn(r0 - __low2float(m), r1 - __high2float(m));
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  mid = *reinterpret_cast<const uint32_t*>(&m);
+  lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+// acc (16 x 8 tile nt) += A B for the A fragment given as values: row g
+// (x[0..1] at k 2t, 2t+1; x[4..5] at k 2t+8, 2t+9) and row g+8 (x[2..3],
+// x[6..7]); B from the bf16 rows of w (row stride ws) at k0.
+__device__ __forceinline__ void mma_split(float (&acc)[4][4], const float (&x)[8],
+                                          const __nv_bfloat16* w, int ws, int k0, int g, int t) {
+  uint32_t ah[4], am[4], al[4];
+  split3(x[0], x[1], ah[0], am[0], al[0]);
+  split3(x[2], x[3], ah[1], am[1], al[1]);
+  split3(x[4], x[5], ah[2], am[2], al[2]);
+  split3(x[6], x[7], ah[3], am[3], al[3]);
 #pragma unroll
-    for (int c = 0; c < kHid; ++c) acc = fmaf(W2[r * kHid + c], h1[c], acc);
-    out = fmaf(W3[r], fmaxf(acc, 0.f), out);
+  for (int nt = 0; nt < 4; ++nt) {
+    const __nv_bfloat16* row = w + (nt * 8 + g) * ws + k0 + 2 * t;
+    const uint32_t b0 = *reinterpret_cast<const uint32_t*>(row);
+    const uint32_t b1 = *reinterpret_cast<const uint32_t*>(row + 8);
+    mma_bf16(acc[nt], al, b0, b1);  // small terms first
+    mma_bf16(acc[nt], am, b0, b1);
+    mma_bf16(acc[nt], ah, b0, b1);
   }
-  L.p3[i + L.px * j + L.plane * k] = out * (s > 0.f ? s : 1.f);
+}
+
+// The layer nodes, 16 per warp and step of its loop: the inputs of the 16
+// nodes are gathered into a shared tile (two lanes per node), scaled by
+// 1/s, and the two hidden layers run as MMAs whose accumulators stay in
+// registers (layer 1's output fragments are layer 2's A operand); the
+// output layer is a dot product reduced over the four lanes of a row.
+__global__ void __launch_bounds__(32 * kWarps) learned_layer(LearnedParams L) {
+  __shared__ __align__(16) __nv_bfloat16 w1s[kHid * kWS1];
+  __shared__ __align__(16) __nv_bfloat16 w2s[kHid * kWS2];
+  __shared__ float b1s[kHid], b2s[kHid], w3s[kHid];
+  __shared__ __align__(16) float xs[kWarps][16 * kXS];
+  __shared__ float ss[kWarps][16];
+  const int K = L.nin, KP = (K + 15) / 16 * 16;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const __nv_bfloat16* W1 = L.w;
+  const __nv_bfloat16* W2 = W1 + kHid * K + kHid;
+  for (int e = tid; e < kHid * kWS1; e += 32 * kWarps) {
+    const int n = e / kWS1, c = e % kWS1;
+    w1s[e] = c < K ? W1[n * K + c] : __float2bfloat16(0.f);
+  }
+  for (int e = tid; e < kHid * kWS2; e += 32 * kWarps) {
+    const int n = e / kWS2, c = e % kWS2;
+    w2s[e] = c < kHid ? W2[n * kHid + c] : __float2bfloat16(0.f);
+  }
+  for (int e = tid; e < kHid; e += 32 * kWarps) {
+    b1s[e] = __bfloat162float(W1[kHid * K + e]);
+    b2s[e] = __bfloat162float(W2[kHid * kHid + e]);
+    w3s[e] = __bfloat162float(W2[kHid * kHid + kHid + e]);
+  }
+  float* X = xs[warp];
+  for (int e = lane; e < 16 * kXS; e += 32) X[e] = 0.f;  // the padding columns stay 0
+  __syncthreads();
+  const float b3 = __bfloat162float(W2[kHid * kHid + 2 * kHid]);
+  const int nv = L.ndim == 3 ? 3 : 1;
+  const int nfield = K - 1;  // inputs from the field; the last one is r
+  const int g = lane >> 2, t = lane & 3;
+  const int n = lane & 15, h = lane >> 4;  // gather: node n of the group, half h
+  const float* lv[3] = {L.p0, L.p1, L.p2};
+  const int nn[3] = {L.nx, L.ny, L.nz};
+  const int64_t stride[3] = {1, L.px, L.plane};
+  for (int grp = blockIdx.x * kWarps + warp; grp * 16 < L.nlayer; grp += gridDim.x * kWarps) {
+    // gather the raw inputs of node n (this lane: every other one)
+    const int m = grp * 16 + n;
+    const bool valid = m < L.nlayer;
+    const int4 nd = valid ? L.layer[m] : make_int4(1, 1, 1, 1);
+    const int ax = nd.w >> 1, sg = (nd.w & 1) ? 1 : -1;
+    int t1 = -1, t2 = -1;  // the transverse axes in increasing order
+    for (int a = 0; a < L.ndim; ++a)
+      if (a != ax) (t1 < 0 ? t1 : t2) = a;
+    const int c[3] = {nd.x, nd.y, nd.z};
+    const int64_t o = nd.x + L.px * nd.y + L.plane * nd.z;
+    float smax = 0.f;
+    for (int f = h; f < nfield; f += 2) {
+      const int wq = f % nv - (nv == 3 ? 1 : 0);
+      const int rest = f / nv;
+      const int v = rest % 3 - 1, u = (rest / 3) % 3 - 1, lvl = rest / 9;
+      int d[3] = {0, 0, 0};
+      d[ax] = sg * u;
+      d[t1] = v;
+      if (t2 >= 0) d[t2] = wq;
+      bool inside = valid;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int q = c[a] + d[a];
+        inside = inside && (a >= L.ndim || (q >= 1 && q <= nn[a] - 2));
+      }
+      const float val =
+          inside ? lv[lvl][o + d[0] * stride[0] + d[1] * stride[1] + d[2] * stride[2]] : 0.f;
+      X[n * kXS + f] = val;
+      smax = fmaxf(smax, fabsf(val));
+    }
+    smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, 16));
+    const float inv = smax > 0.f ? 1.f / smax : 1.f;
+    for (int f = h; f < nfield; f += 2) X[n * kXS + f] *= inv;
+    if (h == 0) {
+      X[n * kXS + nfield] = valid ? sqrtf(L.F[o]) * L.inv_d[ax] : 0.f;  // Courant number
+      ss[warp][n] = smax;
+    }
+    __syncwarp();
+    // layer 1: 16 x KP by KP x 32
+    float acc[4][4];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      acc[nt][0] = acc[nt][2] = b1s[nt * 8 + 2 * t];
+      acc[nt][1] = acc[nt][3] = b1s[nt * 8 + 2 * t + 1];
+    }
+    for (int k0 = 0; k0 < KP; k0 += 16) {
+      const float2 r0 = *reinterpret_cast<const float2*>(X + g * kXS + k0 + 2 * t);
+      const float2 r1 = *reinterpret_cast<const float2*>(X + (g + 8) * kXS + k0 + 2 * t);
+      const float2 r2 = *reinterpret_cast<const float2*>(X + g * kXS + k0 + 2 * t + 8);
+      const float2 r3 = *reinterpret_cast<const float2*>(X + (g + 8) * kXS + k0 + 2 * t + 8);
+      const float xa[8] = {r0.x, r0.y, r1.x, r1.y, r2.x, r2.y, r3.x, r3.y};
+      mma_split(acc, xa, w1s, kWS1, k0, g, t);
+    }
+    // layer 2: the ReLU'd accumulators are the A operand (k block kb = the
+    // n tiles 2kb, 2kb + 1)
+    float acc2[4][4];
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      acc2[nt][0] = acc2[nt][2] = b2s[nt * 8 + 2 * t];
+      acc2[nt][1] = acc2[nt][3] = b2s[nt * 8 + 2 * t + 1];
+    }
+#pragma unroll
+    for (int kb = 0; kb < 2; ++kb) {
+      const float* lo = acc[2 * kb];
+      const float* hi = acc[2 * kb + 1];
+      const float xa[8] = {fmaxf(lo[0], 0.f), fmaxf(lo[1], 0.f), fmaxf(lo[2], 0.f),
+                           fmaxf(lo[3], 0.f), fmaxf(hi[0], 0.f), fmaxf(hi[1], 0.f),
+                           fmaxf(hi[2], 0.f), fmaxf(hi[3], 0.f)};
+      mma_split(acc2, xa, w2s, kWS2, kb * 16, g, t);
+    }
+    // output layer: rows g and g + 8, reduced over the row's four lanes
+    float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt) {
+      const float wa = w3s[nt * 8 + 2 * t], wb = w3s[nt * 8 + 2 * t + 1];
+      y0 = fmaf(wa, fmaxf(acc2[nt][0], 0.f), fmaf(wb, fmaxf(acc2[nt][1], 0.f), y0));
+      y1 = fmaf(wa, fmaxf(acc2[nt][2], 0.f), fmaf(wb, fmaxf(acc2[nt][3], 0.f), y1));
+    }
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 1);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 1);
+    y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+    y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+    if (t == 0) {
+#pragma unroll
+      for (int rr = 0; rr < 2; ++rr) {
+        const int row = g + 8 * rr, mr = grp * 16 + row;
+        if (mr < L.nlayer) {
+          const int4 q = L.layer[mr];
+          const float sc = ss[warp][row];
+          L.p3[q.x + L.px * q.y + L.plane * q.z] = ((rr ? y1 : y0) + b3) * (sc > 0.f ? sc : 1.f);
+        }
+      }
+    }
+    __syncwarp();  // the tile and ss are rewritten by the next group
+  }
 }
 
 __global__ void learned_io(float* __restrict__ p3, const int64_t* __restrict__ snode, int32_t nsrc,
@@ -246,6 +370,38 @@ int awc_forward_learned(awc_ctx* ctx, const awc_problem* p, const double* vel,
   for (int64_t r = 0; r < p->nrec; ++r)
     if (!node(posrecs, p->nrec, r, &rn[r]))
       return awc::fail(ctx, AWC_ERR_INVALID, "receivers must be interior nodes");
+  // the layer nodes by layer_side's rule (nearest absorbing side, x before y
+  // before z, left before right on ties), in memory order
+  std::vector<int4> lay;
+  {
+    const int64_t W = p->halo;
+    const bool ytop = !p->freetop;
+    for (int64_t k = p->ndim == 3 ? 1 : 0; k <= (p->ndim == 3 ? nz - 2 : 0); ++k)
+      for (int64_t j = 1; j <= p->ny - 2; ++j) {
+        const bool near = (ytop && j <= W) || j >= p->ny - 1 - W ||
+                          (p->ndim == 3 && (k <= W || k >= nz - 1 - W));
+        for (int64_t i = 1; i <= p->nx - 2; ++i) {
+          if (!near && i > W && i < p->nx - 1 - W) i = p->nx - 1 - W;  // skip the middle
+          const int64_t c[3] = {i, j, k};
+          int64_t best = W + 1;
+          int ax = 0, sg = 1;
+          for (int a = 0; a < p->ndim; ++a) {
+            const int64_t dl = c[a], dr = n3[a] - 1 - c[a];
+            if (!(a == 1 && p->freetop) && dl < best) {
+              best = dl;
+              ax = a;
+              sg = -1;
+            }
+            if (dr < best) {
+              best = dr;
+              ax = a;
+              sg = 1;
+            }
+          }
+          if (best <= W) lay.push_back(make_int4((int)i, (int)j, (int)k, 2 * ax + (sg > 0)));
+        }
+      }
+  }
   LTRY(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   Mem m;
@@ -253,6 +409,10 @@ int awc_forward_learned(awc_ctx* ctx, const awc_problem* p, const double* vel,
   double* stage;
   int64_t *sn_d, *rn_d;
   __nv_bfloat16* w_d;
+  int4* lay_d;
+  LTRY(ctx, m.get(&lay_d, std::max<size_t>(lay.size(), 1) * sizeof(int4)));
+  if (!lay.empty())
+    LTRY(ctx, cudaMemcpyAsync(lay_d, lay.data(), lay.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
   const int nw = awc_learned_weights_len(p->ndim);
   for (auto& b : buf) {
     LTRY(ctx, m.get(&b, NP * 4));
@@ -294,6 +454,11 @@ int awc_forward_learned(awc_ctx* ctx, const awc_problem* p, const double* vel,
   L.F = F;
   L.w = w_d;
   L.nin = p->ndim == 3 ? 82 : 28;
+  L.layer = lay_d;
+  L.nlayer = (int32_t)lay.size();
+  const unsigned lgrid = (unsigned)std::max<int64_t>(
+      1, std::min<int64_t>(((int64_t)lay.size() + 16 * kWarps - 1) / (16 * kWarps),
+                           (int64_t)ctx->num_sms * 6));
   const dim3 blk(32, 8);
   const dim3 grid((unsigned)((p->nx - 2 + 31) / 32), (unsigned)((p->ny - 2 + 7) / 8),
                   (unsigned)(p->ndim == 3 ? nz - 2 : 1));
@@ -304,7 +469,7 @@ int awc_forward_learned(awc_ctx* ctx, const awc_problem* p, const double* vel,
     L.p2 = buf[(it + 2) % 4];
     L.p3 = buf[(it + 3) % 4];
     learned_interior<<<grid, blk, 0, st>>>(L);
-    learned_layer<<<grid, blk, 0, st>>>(L);
+    if (!lay.empty()) learned_layer<<<lgrid, 32 * kWarps, 0, st>>>(L);
     learned_io<<<1, 32, 0, st>>>(L.p3, sn_d, (int32_t)p->nsrc, stf + it * p->nsrc, rn_d,
                                  (int32_t)p->nrec, tr + it * p->nrec);
   }
