@@ -174,52 +174,62 @@ __global__ void __launch_bounds__(32 * kWarps) learned_layer(LearnedParams L) {
   for (int e = lane; e < 16 * kXS; e += 32) X[e] = 0.f;  // the padding columns stay 0
   __syncthreads();
   const float b3 = __bfloat162float(W2[kHid * kHid + 2 * kHid]);
-  const int nv = L.ndim == 3 ? 3 : 1;
-  const int nfield = K - 1;  // inputs from the field; the last one is r
+  const bool d3 = L.ndim == 3;
+  const int npos = d3 ? 27 : 9;    // block positions per time level
+  const int nfield = 3 * npos;     // inputs from the field; input nfield is r
   const int g = lane >> 2, t = lane & 3;
   const int n = lane & 15, h = lane >> 4;  // gather: node n of the group, half h
-  const float* lv[3] = {L.p0, L.p1, L.p2};
-  const int nn[3] = {L.nx, L.ny, L.nz};
-  const int64_t stride[3] = {1, L.px, L.plane};
   for (int grp = blockIdx.x * kWarps + warp; grp * 16 < L.nlayer; grp += gridDim.x * kWarps) {
-    // gather the raw inputs of node n (this lane: every other one)
+    // gather the raw inputs of node n: this lane takes every other block
+    // position and its three time levels
     const int m = grp * 16 + n;
     const bool valid = m < L.nlayer;
     const int4 nd = valid ? L.layer[m] : make_int4(1, 1, 1, 1);
-    const int ax = nd.w >> 1, sg = (nd.w & 1) ? 1 : -1;
-    int t1 = -1, t2 = -1;  // the transverse axes in increasing order
-    for (int a = 0; a < L.ndim; ++a)
-      if (a != ax) (t1 < 0 ? t1 : t2) = a;
-    const int c[3] = {nd.x, nd.y, nd.z};
+    const int ax = nd.w >> 1;
+    const bool pos = nd.w & 1;
+    // steps along the outward normal (u), the first transverse axis (v) and
+    // the second (w, 3D), and which of the offsets -1, 0, +1 stay inside
+    // the interior (bit e for offset e - 1)
+    const int64_t sx = 1, sy = L.px, sz = L.plane;
+    const int64_t su0 = ax == 0 ? sx : ax == 1 ? sy : sz;
+    const int64_t su = pos ? su0 : -su0;
+    const int64_t sv = ax == 0 ? sy : sx;
+    const int64_t sw = ax == 2 ? sy : sz;
+    auto ok3 = [](int c, int nmax) {  // offsets -1, 0, +1 of c within [1, nmax]
+      return (c - 1 >= 1 ? 1 : 0) | 2 | (c + 1 <= nmax ? 4 : 0);
+    };
+    const int cu = ax == 0 ? nd.x : ax == 1 ? nd.y : nd.z;
+    const int nu = ax == 0 ? L.nx : ax == 1 ? L.ny : L.nz;
+    int mu = ok3(cu, nu - 2);
+    if (!pos) mu = ((mu & 1) << 2) | (mu & 2) | ((mu >> 2) & 1);  // u runs against the axis
+    const int mv = ax == 0 ? ok3(nd.y, L.ny - 2) : ok3(nd.x, L.nx - 2);
+    const int mw = d3 ? (ax == 2 ? ok3(nd.y, L.ny - 2) : ok3(nd.z, L.nz - 2)) : 2;
     const int64_t o = nd.x + L.px * nd.y + L.plane * nd.z;
     float smax = 0.f;
-    for (int f = h; f < nfield; f += 2) {
-      const int wq = f % nv - (nv == 3 ? 1 : 0);
-      const int rest = f / nv;
-      const int v = rest % 3 - 1, u = (rest / 3) % 3 - 1, lvl = rest / 9;
-      int d[3] = {0, 0, 0};
-      d[ax] = sg * u;
-      d[t1] = v;
-      if (t2 >= 0) d[t2] = wq;
-      bool inside = valid;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const int q = c[a] + d[a];
-        inside = inside && (a >= L.ndim || (q >= 1 && q <= nn[a] - 2));
-      }
-      const float val =
-          inside ? lv[lvl][o + d[0] * stride[0] + d[1] * stride[1] + d[2] * stride[2]] : 0.f;
-      X[n * kXS + f] = val;
-      smax = fmaxf(smax, fabsf(val));
+    for (int q = h; q < npos; q += 2) {
+      const int u1 = d3 ? q / 9 : q / 3;
+      const int r1 = d3 ? q - 9 * u1 : q - 3 * u1;
+      const int v1 = d3 ? r1 / 3 : r1;
+      const int w1 = d3 ? r1 - 3 * v1 : 1;
+      const bool in = valid && ((mu >> u1) & (mv >> v1) & (mw >> w1) & 1);
+      const int64_t off = o + (u1 - 1) * su + (v1 - 1) * sv + (d3 ? (w1 - 1) * sw : 0);
+      const float a = in ? L.p0[off] : 0.f;
+      const float b = in ? L.p1[off] : 0.f;
+      const float c = in ? L.p2[off] : 0.f;
+      X[n * kXS + q] = a;
+      X[n * kXS + npos + q] = b;
+      X[n * kXS + 2 * npos + q] = c;
+      smax = fmaxf(smax, fmaxf(fabsf(a), fmaxf(fabsf(b), fabsf(c))));
     }
     smax = fmaxf(smax, __shfl_xor_sync(0xffffffffu, smax, 16));
-    const float inv = smax > 0.f ? 1.f / smax : 1.f;
-    for (int f = h; f < nfield; f += 2) X[n * kXS + f] *= inv;
     if (h == 0) {
       X[n * kXS + nfield] = valid ? sqrtf(L.F[o]) * L.inv_d[ax] : 0.f;  // Courant number
       ss[warp][n] = smax;
     }
     __syncwarp();
+    // the field inputs enter scaled by 1/s of their row (r as it is)
+    const float sg0 = ss[warp][g], sg1 = ss[warp][g + 8];
+    const float inv0 = sg0 > 0.f ? 1.f / sg0 : 1.f, inv1 = sg1 > 0.f ? 1.f / sg1 : 1.f;
     // layer 1: 16 x KP by KP x 32
     float acc[4][4];
 #pragma unroll
@@ -228,11 +238,15 @@ __global__ void __launch_bounds__(32 * kWarps) learned_layer(LearnedParams L) {
       acc[nt][1] = acc[nt][3] = b1s[nt * 8 + 2 * t + 1];
     }
     for (int k0 = 0; k0 < KP; k0 += 16) {
-      const float2 r0 = *reinterpret_cast<const float2*>(X + g * kXS + k0 + 2 * t);
-      const float2 r1 = *reinterpret_cast<const float2*>(X + (g + 8) * kXS + k0 + 2 * t);
-      const float2 r2 = *reinterpret_cast<const float2*>(X + g * kXS + k0 + 2 * t + 8);
-      const float2 r3 = *reinterpret_cast<const float2*>(X + (g + 8) * kXS + k0 + 2 * t + 8);
-      const float xa[8] = {r0.x, r0.y, r1.x, r1.y, r2.x, r2.y, r3.x, r3.y};
+      const int ca = k0 + 2 * t, cb = ca + 8;  // this lane's columns ca, ca + 1, cb, cb + 1
+      const float2 r0 = *reinterpret_cast<const float2*>(X + g * kXS + ca);
+      const float2 r1 = *reinterpret_cast<const float2*>(X + (g + 8) * kXS + ca);
+      const float2 r2 = *reinterpret_cast<const float2*>(X + g * kXS + cb);
+      const float2 r3 = *reinterpret_cast<const float2*>(X + (g + 8) * kXS + cb);
+      auto sc = [&](float v, int col, float inv) { return col < nfield ? v * inv : v; };
+      const float xa[8] = {sc(r0.x, ca, inv0), sc(r0.y, ca + 1, inv0), sc(r1.x, ca, inv1),
+                           sc(r1.y, ca + 1, inv1), sc(r2.x, cb, inv0), sc(r2.y, cb + 1, inv0),
+                           sc(r3.x, cb, inv1), sc(r3.y, cb + 1, inv1)};
       mma_split(acc, xa, w1s, kWS1, k0, g, t);
     }
     // layer 2: the ReLU'd accumulators are the A operand (k block kb = the

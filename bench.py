@@ -473,6 +473,59 @@ def gradient_leg(pkg, ctx, rank, world, timed_host):
                       "under torchrun), max over ranks"}
 
 
+def learned_leg(pkg, ctx):
+    """The learned 4-node layer against the 20-node CPML at config 5's grid
+    sizes (384^3 interior, free top; CPML-20 on 424 x 404 x 424, learned-4 on
+    392 x 388 x 392): device time per step of one shot each (CUDA events
+    around the time loop inside awc_forward_learned and awc_forward; nt = 120,
+    a seeded layered velocity model in 1500-4500 m/s, the MLP with seeded
+    random BF16 weights). Speed only: no learned layer is accepted (every
+    trained candidate is unstable), so no reflected energy is measured."""
+    from acousticwavecpml_b200 import learned as L
+    rng = np.random.default_rng(55)
+    n, nt, d = 384, 120, 10.0
+    out = {"workload": "learned4_vs_cpml20_384cube_1shot_nt120", "nt": nt}
+    for name, halo, learned in (("cpml20", 20, False), ("learned4", 4, True)):
+        shape = (n + 2 * halo, n + halo, n + 2 * halo)
+        tops = np.sort(rng.integers(1, shape[1] - 1, 5))
+        layer_c = 1500.0 + 3000.0 * np.sort(rng.random(6))
+        cy = layer_c[np.searchsorted(tops, np.arange(shape[1]))]
+        vel = np.asfortranarray(np.broadcast_to(cy[None, :, None], shape)
+                                * (1.0 + 0.02 * rng.standard_normal(shape)))
+        S = pkg.Sources([[(shape[0] // 2) * d, (halo + 10) * d, (shape[2] // 2) * d]], [0.04],
+                        [pkg.rickersource1D], 10.0)
+        R = pkg.Receivers([[(halo + 5 + 12 * i) * d, (halo + 5) * d, (shape[2] // 2) * d]
+                           for i in range(30)])
+        s = pkg.prepare(tuple((m - 1) * d for m in shape), None, vel, S, R, halo=halo, ppw=1e-9,
+                        freetop=True, precision="f32", nt=nt)
+        p = s["problem"]
+        if learned:
+            k = L.n_inputs(3)
+            wb = L.to_bf16(L.pack(rng.standard_normal((32, k)) / np.sqrt(k),
+                                  0.05 * rng.standard_normal(32),
+                                  rng.standard_normal((32, 32)) / np.sqrt(32),
+                                  0.05 * rng.standard_normal(32),
+                                  rng.standard_normal(32) / np.sqrt(32) * 0.3, 0.01))
+            run = lambda: L.forward_learned(s, wb, ctx)  # noqa: E731
+        else:
+            tr = np.zeros((p.nt, p.nrec), order="F")
+            run = lambda: ctx.forward(p, s["vel"], s["coeffs"], s["possrcs"],  # noqa: E731
+                                      s["dt2srctf"], s["posrecs"], tr)
+        run()  # warm-up (and the CPML plan's autotuning)
+        ms = []
+        for _ in range(3):
+            run()
+            ms.append(ctx.last_run_ms())
+        out[f"{name}_grid"] = list(shape)
+        out[f"{name}_us_per_step"] = 1e3 * min(ms) / nt
+    out["learned_speedup"] = out["cpml20_us_per_step"] / out["learned4_us_per_step"]
+    out["target_speedup"] = 1.3
+    out["tensor_pipe_active_pct"] = ncu_value("learned_layer_3d_168x164x168",
+                                              "tensor_pipe_active_pct")
+    out["accepted"] = False
+    return out
+
+
 def main():
     args = parse_args()
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
@@ -656,6 +709,8 @@ def main():
             return t
 
         line["gradient"] = gradient_leg(pkg, ctx, rank, world, timed_host)
+        if world == 1:
+            line["learned"] = learned_leg(pkg, ctx)
 
         # ---- full-length errors against the FP64 oracle (N=1) -------------
         if world == 1 and rank == 0 and not args.no_oracle:
