@@ -890,11 +890,10 @@ int ensure_io(awc_plan* P) {
   return AWC_OK;
 }
 
-// Tensor maps of the 3D core kernel: for each rotating field buffer a map
-// with the pcur box ((64 + 2A) x (by + 2) x 1) and one with the pold box
-// (64 x by x 1), and one for fact. Dims (nx, ny, nz), pitched strides.
 // Tensor map of a pitched field of the plan for the core kernel at the
-// current tile height: the box with its ring (ring = true) or the tile.
+// current tile height: the pcur box with its ring ((64 + 2A) x (by + 2) x 1,
+// ring = true) or the pold / fact tile (64 x by x 1). Dims (nx, ny, nz),
+// pitched strides.
 bool field_map(const awc_plan* P, CUtensorMap* m, const void* base, bool ring) {
   PFN_cuTensorMapEncodeTiled_v12000 enc = awc::tensor_map_encoder();
   if (!enc) return false;
@@ -912,6 +911,8 @@ bool field_map(const awc_plan* P, CUtensorMap* m, const void* base, bool ring) {
              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor maps of the 3D core kernel: both boxes for each rotating field
+// buffer, and the tile of fact.
 int ensure_maps(awc_plan* P) {
   if (P->maps_by == P->by) return AWC_OK;
   awc_ctx* C = P->ctx;
