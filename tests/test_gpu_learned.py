@@ -1,8 +1,8 @@
 """The learned thin layer (awc_forward_learned) against the numpy FP64
 restatement in oracle/learned_oracle.py: relative L2 <= 1e-4 on traces and
-field (FP32 GPU against FP64), 2D and 3D, free top on and off, with random
-BF16 weights (the solve must reproduce the scheme for any weights) and with
-the shipped trained weights in 2D."""
+field (FP32 GPU against FP64), 2D and 3D, free top on and off, layer widths
+1, 2, 4 and 8, with random BF16 weights (the solve must reproduce the scheme
+for any weights) and with the shipped trained weights in 2D."""
 import os
 import sys
 
@@ -29,9 +29,13 @@ def _random_weights(L, ndim, rng):
     return L.to_bf16(flat)
 
 
-@pytest.mark.parametrize("ndim,freetop,trained", [(2, True, False), (2, False, False),
-                                                  (3, True, False), (2, True, True)])
-def test_learned_layer_vs_oracle(pkg, ctx, ndim, freetop, trained):
+@pytest.mark.parametrize("ndim,freetop,trained,width", [
+    (2, True, False, 4), (2, False, False, 4), (3, True, False, 4), (2, True, True, 4),
+    (3, False, False, 2),   # every side absorbing, a thin layer
+    (2, False, False, 1),   # one node: every block reaches the rim
+    (2, True, False, 8),    # the widest layer
+])
+def test_learned_layer_vs_oracle(pkg, ctx, ndim, freetop, trained, width):
     from acousticwavecpml_b200 import learned as L
     rng = np.random.default_rng(ndim * 10 + freetop)
     shape = (36, 30) if ndim == 2 else (20, 18, 16)
@@ -46,17 +50,18 @@ def test_learned_layer_vs_oracle(pkg, ctx, ndim, freetop, trained):
     S = pkg.Sources(src, [0.04], [pkg.rickersource1D], 20.0)
     R = pkg.Receivers(recs)
     nt = 120 if ndim == 2 else 80
-    s = pkg.prepare(lengths, None, vel, S, R, halo=4, ppw=1e-9, freetop=freetop,
+    s = pkg.prepare(lengths, None, vel, S, R, halo=width, ppw=1e-9, freetop=freetop,
                     precision="f32", nt=nt)
     wb = L.load_weights() if trained else _random_weights(L, ndim, rng)
     tr, pf = L.forward_learned(s, wb, ctx)
     o = _oracle()
     nodes = lambda pos: [tuple(int(v) - 1 for v in row) for row in pos]
-    tr_o, pf_o = o.forward(s["vel"], s["d"], s["dt"], nt, 4, freetop,
+    tr_o, pf_o = o.forward(s["vel"], s["d"], s["dt"], nt, width, freetop,
                            L.unpack(L.from_bf16(wb), ndim), nodes(s["possrcs"]),
                            s["dt2srctf"], nodes(s["posrecs"]))
     e_t = cases.rel_l2(tr, tr_o)
     e_p = cases.rel_l2(pf, pf_o)
-    print(f"learned {ndim}D freetop={freetop} trained={trained}: traces {e_t:.2e} field {e_p:.2e}")
+    print(f"learned {ndim}D freetop={freetop} trained={trained} width={width}: "
+          f"traces {e_t:.2e} field {e_p:.2e}")
     assert np.abs(tr_o).max() > 0
     assert e_t <= 1e-4 and e_p <= 1e-4
