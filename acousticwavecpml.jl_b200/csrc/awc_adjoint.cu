@@ -98,8 +98,16 @@ struct AdjStep {
   int32_t nbox;
   Box box[27];
   int32_t box_blk[28];
+  // ceil(2^32 / d) for the box width and for its column blocks per plane:
+  // x / d = (x m) >> 32 exactly when x d < 2^32 for every quotient the
+  // kernel forms (fastdiv set; else it divides)
+  uint64_t box_mw[27], box_mncb[27];
+  int32_t fastdiv;
 };
 constexpr int ADJ_GENERIC = 27;
+// with the five tensor maps of the TMA-fed kernel, within the 4 KB of kernel
+// parameters
+static_assert(sizeof(AdjStep<double>) + 5 * 128 <= 4096, "AdjStep too large");
 
 // Element index of entry 0 of the band array (`layers` entries along axis a)
 // at the node (i, j, k), and the step from one entry to the next: x
@@ -281,10 +289,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 4) adj_shell(const _
   const int W = B.x1 - B.x0 + 1, ncol = W * (B.y1 - B.y0 + 1);
   const int ncb = (ncol + 255) / 256;
   const int r = blk - A.box_blk[b];
-  const int kz = r / ncb;
+  const int kz = A.fastdiv ? (int)(((uint64_t)r * A.box_mncb[b]) >> 32) : r / ncb;
   const int l = (r - kz * ncb) * 256 + threadIdx.x;
   if (l >= ncol) return;
-  const int jl = l / W;
+  const int jl = A.fastdiv ? (int)(((uint64_t)l * A.box_mw[b]) >> 32) : l / W;
   const int i = B.x0 + (l - jl * W), j = B.y0 + jl, k = ND == 3 ? B.z0 + kz : 0;
 #define AWC_SHELL(zx, zy, zz) \
   case (zx) + 3 * (zy) + 9 * (zz): adj_shell_node<T, I, ND, GRAD, zx, zy, zz>(A, i, j, k); break;
@@ -803,10 +811,16 @@ void adj_regions(awc::AdjStep<T>& A, int ndim) {
           if (zx || zy || zz) add(zx, zy, zz, zx + 3 * zy + 9 * zz);
   }
   A.box_blk[0] = 0;
+  A.fastdiv = 1;
   for (int b = 0; b < A.nbox; ++b) {
     const awc::Box& B = A.box[b];
-    const int64_t ncol = (int64_t)(B.x1 - B.x0 + 1) * (B.y1 - B.y0 + 1);
-    A.box_blk[b + 1] = (int32_t)(A.box_blk[b] + (ncol + 255) / 256 * (B.z1 - B.z0 + 1));
+    const int64_t W = B.x1 - B.x0 + 1, ncol = W * (B.y1 - B.y0 + 1);
+    const int64_t ncb = (ncol + 255) / 256, nbz = B.z1 - B.z0 + 1;
+    A.box_blk[b + 1] = (int32_t)(A.box_blk[b] + ncb * nbz);
+    A.box_mw[b] = ((1ull << 32) + (uint64_t)W - 1) / (uint64_t)W;
+    A.box_mncb[b] = ((1ull << 32) + (uint64_t)ncb - 1) / (uint64_t)ncb;
+    // quotients l / W with l < 256 ncb and r / ncb with r < ncb nbz
+    if (256 * ncb * W >= (1ll << 32) || ncb * nbz * ncb >= (1ll << 32)) A.fastdiv = 0;
   }
   for (int b = A.nbox; b < 27; ++b) A.box_blk[b + 1] = A.box_blk[b];
 }
