@@ -45,14 +45,12 @@ def misfit_gradient(s, observed, checkpoint_every=50, ctx=None):
     return float(J.value), grad, traces
 
 
-def misfit_gradient_shots(setups, observed, checkpoint_every=50, ctx=None):
-    """(Σ J, Σ dJ/dc²) over shots of one model, equal to summing
-    misfit_gradient over the shots in order. setups[s] is shot s's prepare()
-    dict: all share the problem, vel, coeffs and receivers, and only their
-    sources differ. observed: one (nt x nrec) array per shot, or all of them
-    as one (nt x nrec x nshot) array (used without a copy when it is a
-    Fortran-ordered float64 array)."""
-    ctx = ctx or default_context()
+def stack_shots(setups, observed):
+    """The stacked inputs of awc_misfit_gradient_shots, checked: (possrcs
+    (nsrc, ndim, nshot) int64, dt2srctf (nt, nsrc, nshot), observed (nt,
+    nrec, nshot)), Fortran-ordered, so that shot s's block starts at
+    s * nsrc * ndim, s * nt * nsrc and s * nt * nrec. Raises ValueError when
+    the shots do not share the problem, vel, coeffs and receivers."""
     if not setups:
         raise ValueError("no shots")
     s0 = setups[0]
@@ -81,6 +79,20 @@ def misfit_gradient_shots(setups, observed, checkpoint_every=50, ctx=None):
                                      axis=-1))
     stf = np.asfortranarray(np.stack([np.asarray(s["dt2srctf"], dtype=np.float64)
                                       for s in setups], axis=-1))
+    return pos, stf, obs
+
+
+def misfit_gradient_shots(setups, observed, checkpoint_every=50, ctx=None):
+    """(Σ J, Σ dJ/dc²) over shots of one model, equal to summing
+    misfit_gradient over the shots in order. setups[s] is shot s's prepare()
+    dict: all share the problem, vel, coeffs and receivers, and only their
+    sources differ. observed: one (nt x nrec) array per shot, or all of them
+    as one (nt x nrec x nshot) array (used without a copy when it is a
+    Fortran-ordered float64 array)."""
+    pos, stf, obs = stack_shots(setups, observed)
+    ctx = ctx or default_context()
+    s0 = setups[0]
+    p = s0["problem"]
     grad = np.zeros(s0["vel"].shape, order="F")
     J = ctypes.c_double(0.0)
     check(_lib.lib().awc_misfit_gradient_shots(ctx.handle, ctypes.byref(p), len(setups),
