@@ -285,8 +285,10 @@ int awc_forward_batch(awc_ctx* ctx, int32_t nmodels, const awc_problem* models,
  * shot described like awc_forward, and dJ/d(c²) per node (nx*ny[*nz],
  * column-major, 0 on the rim). The forward state is saved every
  * `checkpoint_every` steps and each segment is recomputed once during the
- * backward pass (memory: nt / checkpoint_every saved states plus
- * checkpoint_every + 2 pressure fields). `traces` (nt x nrec) may be NULL. */
+ * backward pass, the next one beside the current one's adjoint steps
+ * (memory: nt / checkpoint_every saved states plus two sets of
+ * checkpoint_every + 2 pressure fields, one set when a single segment covers
+ * nt). `traces` (nt x nrec) may be NULL. */
 int awc_misfit_gradient(awc_ctx* ctx, const awc_problem* p, const double* vel,
                         const double* coeffs, const int64_t* possrcs, const double* dt2srctf,
                         const int64_t* posrecs, const double* observed, int32_t checkpoint_every,
