@@ -59,37 +59,13 @@ struct LearnedParams {
   int32_t nlayer;
 };
 
-// Depth (1 = next to the rim) of the nearest absorbing side and its axis and
-// outward sign, or 0 when the node is not in the layer.
-__device__ __forceinline__ int layer_side(const LearnedParams& L, int i, int j, int k, int& axis,
-                                          int& sign) {
-  const int c[3] = {i, j, k};
-  const int n[3] = {L.nx, L.ny, L.nz};
-  int best = L.width + 1;
-  for (int a = 0; a < L.ndim; ++a) {
-    const int dl = c[a], dr = n[a] - 1 - c[a];
-    const bool left_abs = !(a == 1 && L.freetop);
-    if (left_abs && dl < best) {
-      best = dl;
-      axis = a;
-      sign = -1;
-    }
-    if (dr < best) {
-      best = dr;
-      axis = a;
-      sign = 1;
-    }
-  }
-  return best <= L.width ? best : 0;
-}
-
+// The leapfrog step at every interior node; the layer kernel, which runs
+// after it, overwrites the layer nodes.
 __global__ void __launch_bounds__(256) learned_interior(LearnedParams L) {
   const int i = 1 + blockIdx.x * 32 + threadIdx.x;
   const int j = 1 + blockIdx.y * 8 + threadIdx.y;
   const int k = L.ndim == 3 ? 1 + blockIdx.z : 0;
   if (i > L.nx - 2 || j > L.ny - 2) return;
-  int ax, sg;
-  if (layer_side(L, i, j, k, ax, sg)) return;
   const int64_t o = i + L.px * j + L.plane * k;
   const float pc = L.p2[o];
   float lap = (L.p2[o + 1] - 2.f * pc + L.p2[o - 1]) * L.inv_d2[0] +
@@ -384,8 +360,8 @@ int awc_forward_learned(awc_ctx* ctx, const awc_problem* p, const double* vel,
   for (int64_t r = 0; r < p->nrec; ++r)
     if (!node(posrecs, p->nrec, r, &rn[r]))
       return awc::fail(ctx, AWC_ERR_INVALID, "receivers must be interior nodes");
-  // the layer nodes by layer_side's rule (nearest absorbing side, x before y
-  // before z, left before right on ties), in memory order
+  // the layer nodes: within `width` of the nearest absorbing side (x before
+  // y before z, left before right on ties), in memory order
   std::vector<int4> lay;
   {
     const int64_t W = p->halo;
